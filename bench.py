@@ -1,0 +1,429 @@
+"""Throughput benchmark of the fused LBM step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: D3Q19 float32, 512^3 nodes, all faces PERIODICAL, tau = 0.6
+(mu = 1/30), Taylor-Green vortex initial field (u0 = 0.05, k = 2 pi / N) --
+the 512^3 D3Q19 point of the throughput sweep.  Metric: million lattice
+updates per second (MLUPS), whole job.  One step = one fused kernel launch
+over the lattice (20.4 GB of populations per step, far above the 126 MB L2,
+so no flush is needed between steps).
+
+For N > 1 (torchrun) every rank advances its own independent lattice
+(replicas: the path has no exchange step); time = max over ranks.
+
+``--impl reference`` times the CPU restatement of the reference's step (the
+oracle, numpy) on the host cores on a bounded 64^3 sample of the same
+workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+Q = 19
+TAU_MU = 1.0 / 30.0
+U0 = 0.05
+BYTES_PER_LU = {"fp32": 2 * Q * 4, "fp16s": 2 * Q * 2, "bf16s": 2 * Q * 2}
+
+
+def metric_name(n, storage):
+    return "MLUPS (D3Q19 %s fused step, %d^3 periodic Taylor-Green)" % (storage, n)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=512, help="nodes per axis")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16s", "bf16s"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-size", type=int, default=64)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (timing only; the data path has no collective)
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        power = [num(r[3]) for r in rows]
+        pmax = max([p for p in power if p is not None] + [0.0])
+        # samples under load: power above 40 % of the peak seen in the window
+        load = [r for r, p in zip(rows, power) if p is not None and p >= 0.4 * pmax] or rows
+        sm = [num(r[1]) for r in load if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples_under_load": len(load), "power_w_max": pmax}
+
+
+# ---------------------------------------------------------------------------
+# the measured path
+# ---------------------------------------------------------------------------
+def taylor_green_soa(lat, torch):
+    """f0 = feq(1, u_TG) (float32 SoA) computed on the device."""
+    from funlbm_b200.flow import equilibrium_soa, make_param, taylor_green_velocity
+
+    param = make_param(Q, lat.device)
+    u = taylor_green_velocity(lat.shape, U0, lat.device)
+    rho = torch.ones(lat.shape + (1,), device=lat.device)
+    f0 = equilibrium_soa(param, u, rho)
+    del u, rho
+    return f0
+
+
+def run_device(args, world, rank, local):
+    import torch
+
+    from funlbm_b200.lattice import Lattice, tau_float32
+
+    n = args.size
+    shape = (n, n, n)
+    lat = Lattice(Q, shape, [11000] * 6, tau_float32(TAU_MU), storage=args.storage,
+                  device="cuda:%d" % local)
+    f0 = taylor_green_soa(lat, torch)
+    lat.init(f0)
+    del f0
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        lat.step(None)
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.5)   # let nvidia-smi start sampling before the timed region
+    ev0.record(stream)
+    for _ in range(args.steps):
+        lat.step(None)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(world, ms)
+    status = lat.read_status()
+    lat.release()
+    del lat
+    torch.cuda.empty_cache()
+    return ms_max, clocks, status
+
+
+def run_e2e(args, world, local):
+    """Same workload through the public API (LBMD3 + Config), with the initial
+    populations uploaded from pinned host memory, the device status word read
+    back every step, and the final density / velocity fields downloaded --
+    all inside the timed region."""
+    import torch
+
+    from funlbm_b200.lattice import Lattice, tau_float32
+    from funlbm_b200.lbm import LBMD3, Config
+
+    n = args.size
+    dev = "cuda:%d" % local
+    tmp = Lattice(Q, (n, n, n), [11000] * 6, tau_float32(TAU_MU), device=dev, allocate=False)
+    f0_dev = taylor_green_soa(tmp, torch)
+    f0_host = torch.empty(f0_dev.shape, dtype=torch.float32, pin_memory=True)
+    f0_host.copy_(f0_dev)
+    del f0_dev, tmp
+    torch.cuda.empty_cache()
+    cfg = Config().from_json({
+        "device": dev, "max_step": 10 ** 9, "log_per_steps": 10 ** 9,
+        "file": {"per_steps": 10 ** 9},
+        "flow": {"size": [n - 1] * 3, "param_type": "D3Q19", "param": {"mu": TAU_MU},
+                 "precision": {"storage": args.storage},
+                 "boundary": {k: {"code": "PERIODICAL"} for k in
+                              ("input", "output", "back", "forward", "bottom", "top")}},
+    })
+    lbm = LBMD3(config=cfg)
+    status_host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    lbm.flow.init()
+    lbm.flow._f.copy_(f0_host.view(Q, -1), non_blocking=True)   # H2D of the initial field
+    lbm.flow.update_u_rou()
+    lbm.flow.cul_equ()
+    lbm.particle_swarm.init()
+    for _ in range(args.steps):
+        lbm.run_step(step=lbm.step)
+        status_host.copy_(lbm.flow.lattice.status, non_blocking=True)   # per-step D2H
+        lbm.step += 1
+    rho = lbm.flow.rou.to("cpu")
+    u = lbm.flow.u.to("cpu")
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    sec = max_over_ranks(world, sec)
+    h2d = f0_host.numel() * 4 / args.steps
+    d2h = (rho.numel() + u.numel()) * 4 / args.steps + 4
+    del lbm, rho, u, f0_host
+    torch.cuda.empty_cache()
+    return sec, h2d, d2h
+
+
+def oracle_workload(n):
+    """The oracle on an n^3 sample of the workload (periodic Taylor-Green)."""
+    from oracle import lbm_oracle as O
+
+    fl = O.OracleFlow(Q, (n - 1,) * 3, TAU_MU, {k: O.PERIODICAL for k in O.FACES})
+    e, w, _ = O.velocity_set(Q)
+    x = np.arange(n)[:, None, None] * (2 * np.pi / n)
+    y = np.arange(n)[None, :, None] * (2 * np.pi / n)
+    z = np.arange(n)[None, None, :] * (2 * np.pi / n)
+    ux = U0 * np.sin(x) * np.cos(y) * np.cos(z)
+    uy = -U0 * np.cos(x) * np.sin(y) * np.cos(z)
+    u = np.stack(np.broadcast_arrays(ux, uy, 0 * ux), -1).astype(np.float32)
+    eu = (u @ e.T.astype(np.float32)) * 3
+    f0 = ((1 + eu + eu * eu / 2 - 1.5 * (u * u).sum(-1, keepdims=True)) * w).astype(np.float32)
+    lbm = O.OracleLBM(fl)
+    lbm.init(f0)
+    return lbm
+
+
+def host_threads():
+    try:
+        from threadpoolctl import threadpool_info
+
+        return max([i.get("num_threads", 1) for i in threadpool_info()] + [1])
+    except Exception:
+        return 1
+
+
+def cpu_baseline(args, seconds=12.0):
+    """The oracle (numpy restatement of the reference's step) on a bounded
+    sample: a cpu_size^3 lattice of the same workload, as many steps as fit
+    in `seconds`."""
+    n = args.cpu_size
+    lbm = oracle_workload(n)
+    lbm.run(1)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        lbm.run(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= args.steps:
+            break
+    cores = host_threads()
+    return {"value": n ** 3 * steps / el / 1e6, "unit": "MLUPS", "cores": cores, "kind": "port",
+            "sample": "oracle (numpy restatement of the reference step), %d^3 nodes, %d steps, "
+                      "%.1f s; elementwise numpy single-threaded, BLAS on %d threads"
+                      % (n, steps, el, cores)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(args):
+    """DRAM bytes per lattice update of the step kernel from a committed ncu
+    capture (profiles/traffic.json), scaled to this lattice; None if absent."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            data = json.load(fh)
+        key = "k_step_q%d_%s" % (Q, args.storage)
+        return float(data[key]["bytes_per_node"]) * args.size ** 3
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def main_reference(args, world, rank):
+    """CPU arm: the oracle port of the reference step, each step one step of a
+    cpu_size^3 sample of the workload, on the host cores."""
+    if rank != 0:
+        return
+    n = args.cpu_size
+    lbm = oracle_workload(n)
+    for _ in range(args.warmup):
+        lbm.run(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        lbm.run(1)
+    el = time.perf_counter() - t0
+    value = n ** 3 * args.steps / el / 1e6
+    cores = host_threads()
+    line = {
+        "impl": "reference", "metric": metric_name(args.size, "fp32"), "value": value,
+        "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (Taylor-Green vortex initial field)",
+        "config": {"workload": "D3Q19 periodic Taylor-Green, tau 0.6; CPU sample %d^3 of the %d^3 "
+                               "workload" % (n, args.size), "sample_nodes": n ** 3},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cores, "kind": "port",
+                         "sample": "oracle numpy restatement of the reference step, %d^3 nodes, "
+                                   "%d timed steps" % (n, args.steps)},
+        "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        main_reference(args, world, rank)
+        return 0
+    import torch
+
+    from funlbm_b200 import build
+
+    build.build()
+    world, rank, local = dist_setup(args)
+    n = args.size
+    ms, clocks, status = run_device(args, world, rank, local)
+    ms_per_step = ms / args.steps
+    nodes = n ** 3
+    value = world * nodes * args.steps / (ms / 1e3) / 1e6
+    peak, peak_kind = measured_peak()
+    bytes_per_launch = BYTES_PER_LU[args.storage] * nodes
+    achieved = bytes_per_launch / (ms_per_step / 1e3) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        sec, h2d, d2h = run_e2e(args, world, local)
+        e2e = {"value": world * nodes * args.steps / sec / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "includes": "public API (LBMD3.run_step) incl. init from a pinned host field, "
+                           "per-step status read-back, final rho/u download"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": metric_name(n, args.storage), "value": value, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.storage == "fp32" else args.storage,
+        "data": "synthetic (Taylor-Green vortex initial field, u0=0.05)",
+        "config": {"workload": "D3Q19 %s, %d^3 nodes, all faces periodic, tau 0.6, Taylor-Green "
+                               "u0=0.05; replicas per GPU" % (args.storage, n),
+                   "nodes_per_gpu": nodes, "parallelism": "replicas",
+                   "l2_flush": "not needed: %.1f GB of populations per step >> 126 MB L2"
+                               % (2 * bytes_per_launch / 2 / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": profiled_traffic(args),
+                     "algorithmic_bytes_per_launch": bytes_per_launch},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks,
+        "device_status": status,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

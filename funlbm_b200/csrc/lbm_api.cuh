@@ -1,0 +1,70 @@
+// Host-side helpers shared by the C-ABI translation units: error reporting,
+// lattice validation, Geom construction, fast index division.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+
+#include "lbm_lattice.cuh"
+
+namespace lbm {
+
+void set_error(const char *fmt, ...);
+int fail_cuda(cudaError_t e, const char *where);
+int check_lattice(const lbm_lattice *lat);  // LBM_OK or an error code (message set)
+Geom make_geom(const lbm_lattice *lat);
+bool any_face(const lbm_lattice *lat, int code);
+
+// Launch-error check after a kernel launch.
+#define LBM_LAUNCH_CHECK(where)                              \
+  do {                                                       \
+    cudaError_t e__ = cudaGetLastError();                    \
+    if (e__ != cudaSuccess) return ::lbm::fail_cuda(e__, where); \
+  } while (0)
+
+// Division of node indices (< 2^31) by a lattice extent d (< 2^31) with one
+// high multiply: m = ceil(2^(31+l) / d), l = ceil(log2 d), so that
+// floor(n / d) = floor(n * m / 2^(31+l)) for every n < 2^31 (the error term
+// n * (m - 2^(31+l)/d) / 2^(31+l) stays below 1/d).
+struct FastDiv {
+  unsigned d, m, s;  // s = l - 1; d == 1 is special-cased with m == 0
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f{d, 0u, 0u};
+  if (d <= 1) return f;
+  unsigned l = 0;
+  while ((1ull << l) < d) ++l;
+  const unsigned long long p = 1ull << (31 + l);
+  f.m = (unsigned)((p + d - 1) / d);
+  f.s = l - 1;
+  return f;
+}
+
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) {
+  return f.m == 0 ? n : (__umulhi(n, f.m) >> f.s);
+}
+
+// (x, y, z) of node idx
+struct NodeDecomp {
+  FastDiv dz, dy;
+  __device__ __forceinline__ void operator()(unsigned idx, int &x, int &y, int &z) const {
+    const unsigned t = fdiv(idx, dz);
+    z = (int)(idx - t * dz.d);
+    const unsigned xx = fdiv(t, dy);
+    y = (int)(t - xx * dy.d);
+    x = (int)xx;
+  }
+};
+
+inline NodeDecomp make_decomp(const Geom &g) {
+  return NodeDecomp{make_fastdiv((unsigned)g.nz), make_fastdiv((unsigned)g.ny)};
+}
+
+inline unsigned blocks_for(long long n, int threads) {
+  return (unsigned)((n + threads - 1) / threads);
+}
+
+}  // namespace lbm

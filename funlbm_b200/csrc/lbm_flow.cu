@@ -1,0 +1,508 @@
+// Flow kernels: initialisation, the fused time step, and the single-function
+// kernels (collide / stream / moments / force) of the reference's FlowD3.
+#include "lbm_api.cuh"
+
+namespace lbm {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Fused step
+// ---------------------------------------------------------------------------
+struct StepArgs {
+  Geom g;
+  NodeDecomp dec;
+  const void *fa;
+  void *fb;
+  float go[3], gn[3];
+  const float *fol_old, *fol_new;
+  const uint8_t *ch_old, *ch_new;
+  const float *face_rho_in;
+  float *face_rho_out;
+  float *obs_f, *obs_rho, *obs_u;
+  unsigned *status;
+};
+
+template <int Q>
+__device__ __forceinline__ void write_face_rho(const Geom &g, float *out, int x, int y, int z,
+                                               float rho) {
+  if (x == 0) out[plane_index(g, 0, x, y, z)] = rho;
+  if (x == g.nx - 1) out[plane_index(g, 1, x, y, z)] = rho;
+  if (y == 0) out[plane_index(g, 2, x, y, z)] = rho;
+  if (y == g.ny - 1) out[plane_index(g, 3, x, y, z)] = rho;
+  if (z == 0) out[plane_index(g, 4, x, y, z)] = rho;
+  if (z == g.nz - 1) out[plane_index(g, 5, x, y, z)] = rho;
+}
+
+// One node per thread, nodes in memory order so that each warp owns one
+// 32-node chunk.  Interior nodes pull with constant offsets; face nodes take
+// the face rules.  FORCE adds cul_equ2 and the second moment pass; without it
+// both are exact no-ops (the reference adds zeros and recomputes identical
+// moments), so they are skipped.
+template <int Q, int S, bool FORCE>
+__global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= (unsigned)a.g.n) return;
+  int x, y, z;
+  a.dec(idx, x, y, z);
+  const bool face = on_any_face(a.g, x, y, z);
+  const T *__restrict__ fa = static_cast<const T *>(a.fa);
+  float f[Q];
+  if (!face)
+    pull_interior<Q, S>(fa, a.g, idx, f);
+  else
+    pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
+
+  float fox = a.go[0], foy = a.go[1], foz = a.go[2];
+  float fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
+  if (a.fol_old != nullptr && (a.ch_old == nullptr || a.ch_old[idx >> 5])) {
+    fox += a.fol_old[3ull * idx];
+    foy += a.fol_old[3ull * idx + 1];
+    foz += a.fol_old[3ull * idx + 2];
+  }
+  if (a.fol_new != nullptr && (a.ch_new == nullptr || a.ch_new[idx >> 5])) {
+    fnx += a.fol_new[3ull * idx];
+    fny += a.fol_new[3ull * idx + 1];
+    fnz += a.fol_new[3ull * idx + 2];
+  }
+  float rho, ux, uy, uz;
+  moments<Q>(f, fox, foy, foz, face, rho, ux, uy, uz);
+  if (FORCE) {
+    add_force<Q>(f, a.g, ux, uy, uz, fnx, fny, fnz);
+    moments<Q>(f, fnx, fny, fnz, face, rho, ux, uy, uz);
+  }
+  flag_bad(a.status, rho, ux, uy, uz);
+  if (face && a.face_rho_out != nullptr) write_face_rho<Q>(a.g, a.face_rho_out, x, y, z, rho);
+  if (a.obs_f != nullptr) {
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      a.obs_f[(long long)i * a.g.n + idx] = f[i];
+    });
+  }
+  if (a.obs_rho != nullptr) a.obs_rho[idx] = rho;
+  if (a.obs_u != nullptr) {
+    a.obs_u[3ull * idx] = ux;
+    a.obs_u[3ull * idx + 1] = uy;
+    a.obs_u[3ull * idx + 2] = uz;
+  }
+  if (a.fb != nullptr) {
+    collide<Q>(f, a.g, rho, ux, uy, uz);
+    T *__restrict__ fb = static_cast<T *>(a.fb);
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      St::store(fb + (long long)i * a.g.n + idx, f[i], V::w(i));
+    });
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Initialisation: f = f0 (or w), moments with FOL = 0 and the face rule,
+// then two collisions with those same moments (LBMD3._init's cul_equ and
+// step 1's cul_equ, which the reference runs before refreshing the moments).
+// ---------------------------------------------------------------------------
+template <int Q, int S>
+__global__ void __launch_bounds__(kThreads)
+    k_init(const Geom g, const NodeDecomp dec, const float *f0, void *fa_, float *face_rho) {
+  using V = VSet<Q>;
+  using St = Storage<S>;
+  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= (unsigned)g.n) return;
+  int x, y, z;
+  dec(idx, x, y, z);
+  const bool face = on_any_face(g, x, y, z);
+  float f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = f0 ? f0[(long long)i * g.n + idx] : V::w(i);
+  float rho, ux, uy, uz;
+  moments<Q>(f, 0.f, 0.f, 0.f, face, rho, ux, uy, uz);
+  collide<Q>(f, g, rho, ux, uy, uz);
+  collide<Q>(f, g, rho, ux, uy, uz);
+  if (face && face_rho != nullptr) write_face_rho<Q>(g, face_rho, x, y, z, rho);
+  typename St::T *fa = static_cast<typename St::T *>(fa_);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) St::store(fa + (long long)i * g.n + idx, f[i], V::w(i));
+}
+
+// ---------------------------------------------------------------------------
+// Single-function kernels (float32 SoA), one reference method each.
+// ---------------------------------------------------------------------------
+template <int Q>
+__global__ void __launch_bounds__(kThreads)
+    k_collide(const Geom g, float *f, const float *rho, const float *u, float *feq) {
+  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= (unsigned)g.n) return;
+  const float r = rho[idx], ux = u[3ull * idx], uy = u[3ull * idx + 1], uz = u[3ull * idx + 2];
+  const float u2 = (ux * ux + uy * uy + uz * uz) * 0.5f * g.inv_cs2;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const long long k = (long long)i * g.n + idx;
+    const float fe = feq_of<Q>(g, i, r, ux, uy, uz, u2);
+    if (feq != nullptr) feq[k] = fe;
+    f[k] = f[k] - (f[k] - fe) * g.inv_tau;
+  }
+}
+
+// f_stream + f_stream_bound_* with every face code, NON_EQUILIBRIUM included.
+template <int Q>
+__global__ void __launch_bounds__(kThreads) k_stream(const Geom g, const NodeDecomp dec,
+                                                     const float *fin, float *fout,
+                                                     const float *rho, const float *feq) {
+  using V = VSet<Q>;
+  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= (unsigned)g.n) return;
+  int x, y, z;
+  dec(idx, x, y, z);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    int fc = -1;
+    if (x == 0 && (V::ex(i) > 0 || g.face[0] == LBM_BC_NON_EQUILIBRIUM)) fc = 0;
+    if (x == g.nx - 1 && (V::ex(i) < 0 || g.face[1] == LBM_BC_NON_EQUILIBRIUM)) fc = 1;
+    if (V::ey(i) > 0 && y == 0) fc = 2;
+    if (V::ey(i) < 0 && y == g.ny - 1) fc = 3;
+    if (V::ez(i) > 0 && z == 0) fc = 4;
+    if (V::ez(i) < 0 && z == g.nz - 1) fc = 5;
+    float v;
+    if (fc < 0) {
+      v = fin[(long long)i * g.n + idx - ((long long)V::ex(i) * g.nyz + (long long)V::ey(i) * g.nz +
+                                          V::ez(i))];
+    } else {
+      const int code = g.face[fc];
+      if (code == LBM_BC_PERIODICAL) {
+        int sx = x, sy = y, sz = z;
+        const bool first = (fc & 1) == 0;
+        if ((fc >> 1) == 0) sx = first ? g.nx - 1 : 0;
+        else if ((fc >> 1) == 1) sy = first ? g.ny - 1 : 0;
+        else sz = first ? g.nz - 1 : 0;
+        v = fin[(long long)i * g.n + ((long long)sx * g.ny + sy) * g.nz + sz];
+      } else if (code == LBM_BC_NON_EQUILIBRIUM) {
+        const int nbx = fc == 0 ? 1 : g.nx - 2;
+        const long long nb = ((long long)nbx * g.ny + y) * g.nz + z;
+        const float rolled = pull_rolled<Q, LBM_STORAGE_FP32>(fin, g, i, nbx, y, z);
+        v = feq[(long long)i * g.n + idx] + (rolled - feq[(long long)i * g.n + nb]);
+      } else {
+        v = fin[(long long)V::rev(i) * g.n + idx];
+        if (code == LBM_BC_WALL_WITH_SPEED) {
+          const float eu = (float)V::ex(i) * g.uw[fc][0] + (float)V::ey(i) * g.uw[fc][1] +
+                           (float)V::ez(i) * g.uw[fc][2];
+          v -= 2.f * (rho[idx] * V::w(i)) * eu * g.inv_cs2;
+        }
+      }
+    }
+    fout[(long long)i * g.n + idx] = v;
+  }
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(float *addr, float v) {
+  if (v >= 0.f) atomicMax(reinterpret_cast<int *>(addr), __float_as_int(v));
+}
+
+template <int Q>
+__global__ void __launch_bounds__(kThreads)
+    k_moments(const Geom g, const NodeDecomp dec, const float *f, const float *fol, float *rho,
+              float *u, float *p, float *rmax) {
+  __shared__ float s_max[kThreads / 32];
+  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
+  float r = 0.f;
+  if (idx < (unsigned)g.n) {
+    int x, y, z;
+    dec(idx, x, y, z);
+    float fl[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) fl[i] = f[(long long)i * g.n + idx];
+    const float fx = fol ? fol[3ull * idx] : 0.f, fy = fol ? fol[3ull * idx + 1] : 0.f,
+                fz = fol ? fol[3ull * idx + 2] : 0.f;
+    float ux, uy, uz;
+    moments<Q>(fl, fx, fy, fz, on_any_face(g, x, y, z), r, ux, uy, uz);
+    rho[idx] = r;
+    if (p != nullptr) p[idx] = r / 3.0f;
+    u[3ull * idx] = ux;
+    u[3ull * idx + 1] = uy;
+    u[3ull * idx + 2] = uz;
+  }
+  if (rmax == nullptr) return;  // uniform per launch
+  for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float m = threadIdx.x < kThreads / 32 ? s_max[threadIdx.x] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) atomic_max_nonneg(rmax, m);
+  }
+}
+
+// update_u_rou_boundary's NON_EQUILIBRIUM part (flow/d3/base.py:135-148): the
+// inlet takes the duct profile scaled by Re mu / max(rho) / min(Y, Z) and the
+// density of plane 1; the outlet copies plane X-2.  One thread per (y, z).
+__global__ void k_neq_moments(const Geom g, float *rho, float *u, const float *rmax) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nyz) return;
+  const long long plane = g.nyz;
+  if (g.face[0] == LBM_BC_NON_EQUILIBRIUM) {
+    const float uw = (1.0f / *rmax) * g.re_mu / (float)(g.ny < g.nz ? g.ny : g.nz);
+    u[3 * t] = (float)((double)uw * g.neq_profile[t]);
+    rho[t] = rho[plane + t];
+  }
+  if (g.face[1] == LBM_BC_NON_EQUILIBRIUM) {
+    const long long last = (long long)(g.nx - 1) * plane + t, prev = last - plane;
+    rho[last] = rho[prev];
+    for (int k = 0; k < 3; ++k) u[3 * last + k] = u[3 * prev + k];
+  }
+}
+
+template <int Q>
+__global__ void __launch_bounds__(kThreads)
+    k_force(const Geom g, float *f, const float *u, const float *fol) {
+  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= (unsigned)g.n) return;
+  float fl[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fl[i] = f[(long long)i * g.n + idx];
+  add_force<Q>(fl, g, u[3ull * idx], u[3ull * idx + 1], u[3ull * idx + 2], fol[3ull * idx],
+               fol[3ull * idx + 1], fol[3ull * idx + 2]);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[(long long)i * g.n + idx] = fl[i];
+}
+
+// ---------------------------------------------------------------------------
+// Dispatch helpers
+// ---------------------------------------------------------------------------
+template <template <int> class F, typename... A>
+int dispatch_q(int q, A &&...args) {
+  switch (q) {
+    case 13: return F<13>::run(args...);
+    case 15: return F<15>::run(args...);
+    case 19: return F<19>::run(args...);
+    case 27: return F<27>::run(args...);
+    default: set_error("Unknown parameter type: D3Q%d", q); return LBM_ERR_INVALID;
+  }
+}
+
+template <int Q>
+struct RunStep {
+  template <int S>
+  static void go(const StepArgs &a, bool force, cudaStream_t s) {
+    const unsigned nb = blocks_for(a.g.n, kThreads);
+    if (force)
+      k_step<Q, S, true><<<nb, kThreads, 0, s>>>(a);
+    else
+      k_step<Q, S, false><<<nb, kThreads, 0, s>>>(a);
+  }
+  static int run(const StepArgs &a, int storage, bool force, cudaStream_t s) {
+    switch (storage) {
+      case LBM_STORAGE_FP32: go<LBM_STORAGE_FP32>(a, force, s); break;
+      case LBM_STORAGE_FP16S: go<LBM_STORAGE_FP16S>(a, force, s); break;
+      default: go<LBM_STORAGE_BF16S>(a, force, s); break;
+    }
+    LBM_LAUNCH_CHECK("lbm_flow_step");
+    return LBM_OK;
+  }
+};
+
+template <int Q>
+struct RunInit {
+  static int run(const Geom &g, const float *f0, void *fa, float *face_rho, int storage,
+                 cudaStream_t s) {
+    const unsigned nb = blocks_for(g.n, kThreads);
+    const NodeDecomp dec = make_decomp(g);
+    switch (storage) {
+      case LBM_STORAGE_FP32:
+        k_init<Q, LBM_STORAGE_FP32><<<nb, kThreads, 0, s>>>(g, dec, f0, fa, face_rho);
+        break;
+      case LBM_STORAGE_FP16S:
+        k_init<Q, LBM_STORAGE_FP16S><<<nb, kThreads, 0, s>>>(g, dec, f0, fa, face_rho);
+        break;
+      default:
+        k_init<Q, LBM_STORAGE_BF16S><<<nb, kThreads, 0, s>>>(g, dec, f0, fa, face_rho);
+        break;
+    }
+    LBM_LAUNCH_CHECK("lbm_flow_init");
+    return LBM_OK;
+  }
+};
+
+template <int Q>
+struct RunCollide {
+  static int run(const Geom &g, float *f, const float *rho, const float *u, float *feq,
+                 cudaStream_t s) {
+    k_collide<Q><<<blocks_for(g.n, kThreads), kThreads, 0, s>>>(g, f, rho, u, feq);
+    LBM_LAUNCH_CHECK("lbm_collide");
+    return LBM_OK;
+  }
+};
+
+template <int Q>
+struct RunStream {
+  static int run(const Geom &g, const float *fin, float *fout, const float *rho, const float *feq,
+                 cudaStream_t s) {
+    k_stream<Q><<<blocks_for(g.n, kThreads), kThreads, 0, s>>>(g, make_decomp(g), fin, fout, rho,
+                                                               feq);
+    LBM_LAUNCH_CHECK("lbm_stream");
+    return LBM_OK;
+  }
+};
+
+template <int Q>
+struct RunMoments {
+  static int run(const Geom &g, const float *f, const float *fol, float *rho, float *u, float *p,
+                 float *rmax, cudaStream_t s) {
+    k_moments<Q><<<blocks_for(g.n, kThreads), kThreads, 0, s>>>(g, make_decomp(g), f, fol, rho, u,
+                                                                p, rmax);
+    LBM_LAUNCH_CHECK("lbm_moments");
+    return LBM_OK;
+  }
+};
+
+template <int Q>
+struct RunForce {
+  static int run(const Geom &g, float *f, const float *u, const float *fol, cudaStream_t s) {
+    k_force<Q><<<blocks_for(g.n, kThreads), kThreads, 0, s>>>(g, f, u, fol);
+    LBM_LAUNCH_CHECK("lbm_add_force");
+    return LBM_OK;
+  }
+};
+
+}  // namespace lbm
+
+using namespace lbm;
+
+extern "C" {
+
+int lbm_flow_init(const lbm_lattice *lat, const float *f0, void *fa, float *face_rho,
+                  void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if (fa == nullptr) {
+    set_error("lbm_flow_init: population buffer is NULL");
+    return LBM_ERR_INVALID;
+  }
+  if ((any_face(lat, LBM_BC_WALL_WITH_SPEED) || any_face(lat, LBM_BC_NON_EQUILIBRIUM)) &&
+      face_rho == nullptr) {
+    set_error("lbm_flow_init: WALL_WITH_SPEED / NON_EQUILIBRIUM faces need face_rho");
+    return LBM_ERR_INVALID;
+  }
+  const Geom g = make_geom(lat);
+  return dispatch_q<RunInit>(lat->q, g, f0, fa, face_rho, lat->storage, (cudaStream_t)stream);
+}
+
+int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
+                  const float *face_rho_in, float *face_rho_out, const lbm_observe *obs,
+                  uint32_t *status, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if (any_face(lat, LBM_BC_NON_EQUILIBRIUM)) {
+    set_error("lbm_flow_step: NON_EQUILIBRIUM faces need the global inlet density; run them "
+              "through lbm_collide / lbm_stream / lbm_moments / lbm_force");
+    return LBM_ERR_UNSUPPORTED;
+  }
+  if (fa == nullptr) {
+    set_error("lbm_flow_step: input populations are NULL");
+    return LBM_ERR_INVALID;
+  }
+  const bool wws = any_face(lat, LBM_BC_WALL_WITH_SPEED);
+  if (wws && face_rho_in == nullptr) {
+    set_error("lbm_flow_step: WALL_WITH_SPEED faces need face_rho_in");
+    return LBM_ERR_INVALID;
+  }
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = make_geom(lat);
+  a.dec = make_decomp(a.g);
+  a.fa = fa;
+  a.fb = fb;
+  bool use_force = false;
+  if (force != nullptr) {
+    for (int k = 0; k < 3; ++k) {
+      a.go[k] = force->old_uniform[k];
+      a.gn[k] = force->new_uniform[k];
+      use_force = use_force || a.go[k] != 0.f || a.gn[k] != 0.f;
+    }
+    a.fol_old = force->old_field;
+    a.fol_new = force->new_field;
+    a.ch_old = force->old_chunks;
+    a.ch_new = force->new_chunks;
+    use_force = use_force || a.fol_old != nullptr || a.fol_new != nullptr;
+  }
+  a.face_rho_in = face_rho_in;
+  a.face_rho_out = wws ? face_rho_out : nullptr;
+  if (obs != nullptr) {
+    a.obs_f = obs->f;
+    a.obs_rho = obs->rho;
+    a.obs_u = obs->u;
+  }
+  a.status = status;
+  return dispatch_q<RunStep>(lat->q, a, lat->storage, use_force, (cudaStream_t)stream);
+}
+
+int lbm_collide(const lbm_lattice *lat, float *f, const float *rho, const float *u, float *feq,
+                void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if (f == nullptr || rho == nullptr || u == nullptr) {
+    set_error("lbm_collide: f, rho and u are required");
+    return LBM_ERR_INVALID;
+  }
+  return dispatch_q<RunCollide>(lat->q, make_geom(lat), f, rho, u, feq, (cudaStream_t)stream);
+}
+
+int lbm_stream(const lbm_lattice *lat, const float *f_in, float *f_out, const float *rho,
+               const float *feq, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if (f_in == nullptr || f_out == nullptr || f_in == f_out) {
+    set_error("lbm_stream: needs distinct input and output buffers");
+    return LBM_ERR_INVALID;
+  }
+  if (any_face(lat, LBM_BC_WALL_WITH_SPEED) && rho == nullptr) {
+    set_error("lbm_stream: WALL_WITH_SPEED faces need rho");
+    return LBM_ERR_INVALID;
+  }
+  if (any_face(lat, LBM_BC_NON_EQUILIBRIUM) && feq == nullptr) {
+    set_error("lbm_stream: NON_EQUILIBRIUM faces need feq");
+    return LBM_ERR_INVALID;
+  }
+  return dispatch_q<RunStream>(lat->q, make_geom(lat), f_in, f_out, rho, feq,
+                               (cudaStream_t)stream);
+}
+
+int lbm_moments(const lbm_lattice *lat, const float *f, const float *fol, float *rho, float *u,
+                float *p, float *scratch, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if (f == nullptr || rho == nullptr || u == nullptr) {
+    set_error("lbm_moments: f, rho and u are required");
+    return LBM_ERR_INVALID;
+  }
+  const bool neq = any_face(lat, LBM_BC_NON_EQUILIBRIUM);
+  const bool neq_in = lat->face[0] == LBM_BC_NON_EQUILIBRIUM;
+  if (neq_in && scratch == nullptr) {
+    set_error("lbm_moments: a NON_EQUILIBRIUM input face needs one float of scratch");
+    return LBM_ERR_INVALID;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geom g = make_geom(lat);
+  if (neq_in) {
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(float), s);
+    if (e != cudaSuccess) return fail_cuda(e, "lbm_moments");
+  }
+  rc = dispatch_q<RunMoments>(lat->q, g, f, fol, rho, u, p, neq_in ? scratch : nullptr, s);
+  if (rc || !neq) return rc;
+  k_neq_moments<<<blocks_for(g.nyz, 128), 128, 0, s>>>(g, rho, u, scratch);
+  LBM_LAUNCH_CHECK("lbm_moments");
+  return LBM_OK;
+}
+
+int lbm_add_force(const lbm_lattice *lat, float *f, const float *u, const float *fol,
+                  void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if (f == nullptr || u == nullptr || fol == nullptr) {
+    set_error("lbm_add_force: f, u and FOL are required");
+    return LBM_ERR_INVALID;
+  }
+  return dispatch_q<RunForce>(lat->q, make_geom(lat), f, u, fol, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,579 @@
+// Immersed boundary coupling and rigid particles: interpolation (fused with
+// the moment pass it reads), wall spring + Newton-Euler update, spreading,
+// and the rotation-vector marker update.
+#include "lbm_api.cuh"
+
+namespace lbm {
+
+constexpr int kStencil = 64;                // 4 x 4 x 4 nodes per marker
+constexpr int kMarkersPerBlock = 4;         // interpolation / spreading blocks
+constexpr int kIbmThreads = kStencil * kMarkersPerBlock;
+constexpr int kRigidThreads = 256;
+
+// Stencil box of lbm/lbm3d.py:32-44 for marker position `l` on one axis:
+// lo = max(floor(l) - 1, 0), hi = min(lo + 4, size) with size = nodes - 1
+// (the reference clamps to the configured size, so the last node is never
+// part of a stencil).  Computed in float32 like the reference.
+// lo is also capped at size (the box is then empty) so that markers far
+// outside the domain (or non-finite) never produce an out-of-range index.
+__device__ __forceinline__ void box_axis(float l, int size, int &lo, int &hi) {
+  float rl = floorf(l) - 1.f;
+  rl = fmaxf(rl, 0.f);
+  float rr = fminf(rl + 4.f, (float)size);
+  rl = fminf(rl, (float)size);
+  rr = fmaxf(rr, 0.f);
+  lo = (int)rl;
+  hi = (int)rr;
+}
+
+// 4-point cosine delta of lbm/lbm3d.py:46-64, one axis:
+// (1 + cos(|r pi / 2|)) / 4, and the |r| <= 2 test of the mask.
+__device__ __forceinline__ float delta_axis(float r, bool &inside) {
+  inside = inside && (fabsf(r) <= 2.f);
+  const float arg = fabsf(r * 3.14159265358979323846f / 2.f);
+  return (1.f + cosf(arg)) / 4.f;
+}
+
+// Unnormalised weight of stencil slot j of a marker at `l`; false if the slot
+// is outside the (clamped) box.
+__device__ __forceinline__ bool stencil_slot(const Geom &g, const float l[3], int j, int &x, int &y,
+                                             int &z, float &w) {
+  int lo[3], hi[3];
+  box_axis(l[0], g.nx - 1, lo[0], hi[0]);
+  box_axis(l[1], g.ny - 1, lo[1], hi[1]);
+  box_axis(l[2], g.nz - 1, lo[2], hi[2]);
+  x = lo[0] + (j >> 4);
+  y = lo[1] + ((j >> 2) & 3);
+  z = lo[2] + (j & 3);
+  if (x >= hi[0] || y >= hi[1] || z >= hi[2]) return false;
+  bool in = true;
+  const float wx = delta_axis((float)x - l[0], in);
+  const float wy = delta_axis((float)y - l[1], in);
+  const float wz = delta_axis((float)z - l[2], in);
+  w = in ? (wx * wy) * wz : 0.f;
+  return true;
+}
+
+// Sum over the 64 stencil threads of one marker (two warps) via shared memory.
+template <int N>
+__device__ __forceinline__ void stencil_sum(float (&v)[N], float (*sh)[kMarkersPerBlock * 2], int slot,
+                                            int mk) {
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) sh[k][mk * 2 + (slot >> 5)] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = sh[k][mk * 2] + sh[k][mk * 2 + 1];
+}
+
+// ---------------------------------------------------------------------------
+// Interpolation: thread = (marker, stencil slot).
+// ---------------------------------------------------------------------------
+struct InterpArgs {
+  Geom g;
+  const void *fa;
+  const float *u_field, *rho_field;
+  float go[3];
+  const float *fol_old;
+  const float *face_rho_in;
+  lbm_particles p;
+  float dt;
+  int step;
+  unsigned *status;
+};
+
+template <int Q, int S>
+__global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
+  __shared__ float sh[3][kMarkersPerBlock * 2];
+  const int mk = threadIdx.x / kStencil, slot = threadIdx.x % kStencil;
+  const int m = blockIdx.x * kMarkersPerBlock + mk;
+  const bool live = m < a.p.n_markers;
+  float acc[3] = {0.f, 0.f, 0.f};  // sum w, sum w (ux+uy+uz), sum w rho
+  float l[3] = {0.f, 0.f, 0.f};
+  if (live) {
+    l[0] = a.p.lx[3 * m];
+    l[1] = a.p.lx[3 * m + 1];
+    l[2] = a.p.lx[3 * m + 2];
+    int x, y, z;
+    float w;
+    if (stencil_slot(a.g, l, slot, x, y, z, w)) {
+      const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
+      float rho, ux, uy, uz;
+      if (a.fa != nullptr) {
+        const typename Storage<S>::T *fa = static_cast<const typename Storage<S>::T *>(a.fa);
+        float f[Q];
+        pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
+        float fx = a.go[0], fy = a.go[1], fz = a.go[2];
+        if (a.fol_old != nullptr) {
+          fx += a.fol_old[3 * idx];
+          fy += a.fol_old[3 * idx + 1];
+          fz += a.fol_old[3 * idx + 2];
+        }
+        moments<Q>(f, fx, fy, fz, on_any_face(a.g, x, y, z), rho, ux, uy, uz);
+      } else {
+        rho = a.rho_field[idx];
+        ux = a.u_field[3 * idx];
+        uy = a.u_field[3 * idx + 1];
+        uz = a.u_field[3 * idx + 2];
+      }
+      acc[0] = w;
+      acc[1] = w * ((ux + uy) + uz);
+      acc[2] = w * rho;
+    }
+  }
+  stencil_sum<3>(acc, sh, slot, mk);
+  if (!live || slot != 0) return;
+  const float W = acc[0];
+  const float lus = W > 0.f ? acc[1] / W : acc[1];
+  const float lrho = W > 0.f ? acc[2] / W : acc[2];
+  if (!(W > 0.f) && a.step > 100 && a.status != nullptr) atomicOr(a.status, LBM_STATUS_STENCIL_EMPTY);
+  const int pi = a.p.marker_owner[m];
+  const float rx = l[0] - a.p.cx[3 * pi], ry = l[1] - a.p.cx[3 * pi + 1],
+              rz = l[2] - a.p.cx[3 * pi + 2];
+  const float wx = a.p.cw[3 * pi], wy = a.p.cw[3 * pi + 1], wz = a.p.cw[3 * pi + 2];
+  const float v[3] = {a.p.cu[3 * pi] + (wy * rz - wz * ry), a.p.cu[3 * pi + 1] + (wz * rx - wx * rz),
+                      a.p.cu[3 * pi + 2] + (wx * ry - wy * rx)};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    a.p.lu[3 * m + k] = v[k];
+    a.p.lF[3 * m + k] = (2.f * lrho) * (v[k] - lus) / a.dt;
+  }
+  a.p.lrou[m] = lrho;
+}
+
+// ---------------------------------------------------------------------------
+// Wall spring (lbm/lbm3d.py:121-167) + update_from_lar
+// (particle/base/base.py:120-151).  One block per particle.
+// ---------------------------------------------------------------------------
+struct RigidArgs {
+  lbm_particles p;
+  int what;
+  float size[3];
+  float dt, dx, gl, rouf;
+};
+
+__device__ __forceinline__ void argext_merge(float &v, int &i, float v2, int i2, bool want_min) {
+  const bool better = want_min ? (v2 < v || (v2 == v && i2 < i)) : (v2 > v || (v2 == v && i2 < i));
+  if (better) {
+    v = v2;
+    i = i2;
+  }
+}
+
+__global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
+  const int pi = blockIdx.x;
+  const int m0 = a.p.marker_offset[pi], m1 = a.p.marker_offset[pi + 1];
+  __shared__ float s_v[6][kRigidThreads / 32];
+  __shared__ int s_i[6][kRigidThreads / 32];
+  __shared__ int s_ext[6];
+  __shared__ double s_sum[3][kRigidThreads / 32];
+  __shared__ float s_cx[3];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+
+  // -- extreme markers: argmin x,y,z then argmax x,y,z (first index on ties)
+  float v[6];
+  int id[6];
+  for (int k = 0; k < 3; ++k) {
+    v[k] = INFINITY;
+    v[k + 3] = -INFINITY;
+    id[k] = id[k + 3] = 0x7fffffff;
+  }
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    for (int k = 0; k < 3; ++k) {
+      const float c = a.p.lx[3 * m + k];
+      argext_merge(v[k], id[k], c, m, true);
+      argext_merge(v[k + 3], id[k + 3], c, m, false);
+    }
+  }
+  for (int k = 0; k < 6; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const float v2 = __shfl_xor_sync(0xffffffffu, v[k], o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, id[k], o);
+      argext_merge(v[k], id[k], v2, i2, k < 3);
+    }
+    if (lane == 0) {
+      s_v[k][wid] = v[k];
+      s_i[k][wid] = id[k];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && (a.what & RIGID_WALL)) {
+    for (int k = 0; k < 6; ++k) {
+      float bv = s_v[k][0];
+      int bi = s_i[k][0];
+      for (int w = 1; w < kRigidThreads / 32; ++w) argext_merge(bv, bi, s_v[k][w], s_i[k][w], k < 3);
+      s_ext[k] = bi;
+    }
+    bool valid = m1 > m0;
+    for (int k = 0; k < 6; ++k) valid = valid && s_ext[k] >= m0 && s_ext[k] < m1;
+    if (valid) {  // (non-finite positions leave no extreme marker: no spring)
+      // spring force k0 (1 - |x - wall| / (2 dx)), clamped at 0; the indexed
+      // += of the reference reads all six old values and the last write wins
+      const float k0 = 300.f;
+      float d[6], dmax = 0.f;
+      for (int k = 0; k < 6; ++k) {
+        const float c = a.p.lx[3 * s_ext[k] + (k % 3)];
+        const float b = k < 3 ? 0.f : a.size[k - 3];
+        d[k] = fmaxf(k0 * (1.f - fabsf(c - b) / (2.f * a.dx)), 0.f);
+        dmax = fmaxf(dmax, d[k]);
+      }
+      if (dmax != 0.f) {
+        float nv[6][3];
+        for (int k = 0; k < 6; ++k)
+          for (int c = 0; c < 3; ++c) {
+            const float nrm = (c == k % 3) ? (k < 3 ? 1.f : -1.f) : 0.f;
+            nv[k][c] = a.p.lF[3 * s_ext[k] + c] + nrm * d[k];
+          }
+        for (int k = 0; k < 6; ++k)
+          for (int c = 0; c < 3; ++c) a.p.lF[3 * s_ext[k] + c] = nv[k][c];
+      }
+    }
+  }
+  __syncthreads();
+  if (!(a.what & RIGID_UPDATE)) return;
+
+  // -- cF = sum(-lF lm) + (1 - rho_p / rho_f) mass [gl, 0, 0]   (float64 sums)
+  double sf[3] = {0.0, 0.0, 0.0};
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    const double lm = a.p.lm[m];
+    for (int k = 0; k < 3; ++k) sf[k] += -(double)a.p.lF[3 * m + k] * lm;
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) sf[k] += __shfl_xor_sync(0xffffffffu, sf[k], o);
+    if (lane == 0) s_sum[k][wid] = sf[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const float mass = a.p.mass[pi];
+    const float buoy = (float)(1.0 - (double)a.p.rou[pi] / (double)a.rouf) * mass;
+    for (int k = 0; k < 3; ++k) {
+      double t = 0.0;
+      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
+      const float cf = (float)t + (k == 0 ? buoy * a.gl : 0.f);
+      a.p.cF[3 * pi + k] = cf;
+      const float cu = a.p.cu[3 * pi + k] + cf / mass * a.dt;
+      a.p.cu[3 * pi + k] = cu;
+      const float cx = a.p.cx[3 * pi + k] + cu * a.dt;
+      a.p.cx[3 * pi + k] = cx;
+      s_cx[k] = cx;
+    }
+  }
+  __syncthreads();
+
+  // -- cT = -sum((lx - cx) x lF lm)  with the new cx   (float64 sums)
+  double st[3] = {0.0, 0.0, 0.0};
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    const double rx = (double)(a.p.lx[3 * m] - s_cx[0]);
+    const double ry = (double)(a.p.lx[3 * m + 1] - s_cx[1]);
+    const double rz = (double)(a.p.lx[3 * m + 2] - s_cx[2]);
+    const double fx = a.p.lF[3 * m], fy = a.p.lF[3 * m + 1], fz = a.p.lF[3 * m + 2];
+    const double lm = a.p.lm[m];
+    st[0] += (ry * fz - rz * fy) * lm;
+    st[1] += (rz * fx - rx * fz) * lm;
+    st[2] += (rx * fy - ry * fx) * lm;
+  }
+  __syncthreads();
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) st[k] += __shfl_xor_sync(0xffffffffu, st[k], o);
+    if (lane == 0) s_sum[k][wid] = st[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 3; ++k) {
+      double t = 0.0;
+      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
+      const float ct = -(float)t;
+      a.p.cT[3 * pi + k] = ct;
+      a.p.cw[3 * pi + k] = a.p.cw[3 * pi + k] + 0.1f * ct * a.dt / a.p.inertia[3 * pi + k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spreading (lbm/lbm3d.py:102-119)
+// ---------------------------------------------------------------------------
+// Clear the chunks written last time this buffer was used (warp per chunk).
+__global__ void k_spread_clear(long long n, float *field, uint8_t *chunks) {
+  const long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const long long nchunks = (n + 31) >> 5;
+  if (chunk >= nchunks) return;
+  if (chunks[chunk] == 0) return;
+  const long long node = chunk * 32 + lane;
+  if (node < n) {
+    field[3 * node] = 0.f;
+    field[3 * node + 1] = 0.f;
+    field[3 * node + 2] = 0.f;
+  }
+  __syncwarp();
+  if (lane == 0) chunks[chunk] = 0;
+}
+
+struct SpreadArgs {
+  Geom g;
+  lbm_particles p;
+  float *field;
+  uint8_t *chunks;
+  int *owner;
+};
+
+// pass 0: flag chunks and claim nodes (max marker index = last in loop order)
+// pass 1: the owning marker writes w lF lm (reference mode)
+// pass 2: release the claims
+// pass 3: accumulate w lF lm (accumulate mode; flags set as in pass 0)
+template <int PASS>
+__global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
+  __shared__ float sh[1][kMarkersPerBlock * 2];
+  const int mk = threadIdx.x / kStencil, slot = threadIdx.x % kStencil;
+  const int m = blockIdx.x * kMarkersPerBlock + mk;
+  const bool live = m < a.p.n_markers;
+  float l[3] = {0.f, 0.f, 0.f};
+  int x = 0, y = 0, z = 0;
+  float w = 0.f;
+  bool in_box = false;
+  if (live) {
+    l[0] = a.p.lx[3 * m];
+    l[1] = a.p.lx[3 * m + 1];
+    l[2] = a.p.lx[3 * m + 2];
+    in_box = stencil_slot(a.g, l, slot, x, y, z, w);
+  }
+  const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
+  if (PASS == 0 || PASS == 2) {
+    if (!in_box) return;
+    if (PASS == 0) {
+      a.chunks[idx >> 5] = 1;
+      atomicMax(a.owner + idx, m);
+    } else {
+      a.owner[idx] = -1;
+    }
+    return;
+  }
+  // passes 1 and 3 need the normalised weight: sum over the marker's stencil
+  float W[1] = {in_box ? w : 0.f};
+  stencil_sum<1>(W, sh, slot, mk);
+  if (!in_box) return;
+  const float wn = W[0] > 0.f ? w / W[0] : w;
+  const float lm = a.p.lm[m];
+  if (PASS == 1) {
+    if (a.owner[idx] != m) return;
+    for (int k = 0; k < 3; ++k) a.field[3 * idx + k] = (wn * a.p.lF[3 * m + k]) * lm;
+  } else {
+    a.chunks[idx >> 5] = 1;
+    for (int k = 0; k < 3; ++k) atomicAdd(a.field + 3 * idx + k, (wn * a.p.lF[3 * m + k]) * lm);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Marker update (particle/base/base.py:153-156, particle/coord.py:87-108):
+// angle += cw; R from the rotation vector (float64, through the unit
+// quaternion); lx = float32(R X0) + cx.  One block per particle.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles p) {
+  const int pi = blockIdx.x;
+  __shared__ double R[9];
+  __shared__ float c[3];
+  if (threadIdx.x == 0) {
+    double v[3];
+    for (int k = 0; k < 3; ++k) {
+      const float ang = p.angle[3 * pi + k] + p.cw[3 * pi + k];
+      p.angle[3 * pi + k] = ang;
+      v[k] = ang;
+      c[k] = p.cx[3 * pi + k];
+    }
+    const double th = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    double s;
+    if (th <= 1e-3) {
+      const double t2 = th * th;
+      s = 0.5 - t2 / 48.0 + t2 * t2 / 3840.0;
+    } else {
+      s = sin(0.5 * th) / th;
+    }
+    double x = s * v[0], y = s * v[1], z = s * v[2], w = cos(0.5 * th);
+    const double nq = sqrt(x * x + y * y + z * z + w * w);
+    x /= nq;
+    y /= nq;
+    z /= nq;
+    w /= nq;
+    R[0] = 1 - 2 * (y * y + z * z);
+    R[1] = 2 * (x * y - z * w);
+    R[2] = 2 * (x * z + y * w);
+    R[3] = 2 * (x * y + z * w);
+    R[4] = 1 - 2 * (x * x + z * z);
+    R[5] = 2 * (y * z - x * w);
+    R[6] = 2 * (x * z - y * w);
+    R[7] = 2 * (y * z + x * w);
+    R[8] = 1 - 2 * (x * x + y * y);
+  }
+  __syncthreads();
+  const int m0 = p.marker_offset[pi], m1 = p.marker_offset[pi + 1];
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    const double X = p.lagrange[3 * m], Y = p.lagrange[3 * m + 1], Z = p.lagrange[3 * m + 2];
+    for (int k = 0; k < 3; ++k) {
+      const double r = R[3 * k] * X + R[3 * k + 1] * Y + R[3 * k + 2] * Z;
+      p.lx[3 * m + k] = (float)r + c[k];
+    }
+  }
+}
+
+template <int Q>
+struct RunInterp {
+  static int run(const InterpArgs &a, int storage, cudaStream_t s) {
+    const unsigned nb = (unsigned)((a.p.n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
+    switch (storage) {
+      case LBM_STORAGE_FP32: k_interp<Q, LBM_STORAGE_FP32><<<nb, kIbmThreads, 0, s>>>(a); break;
+      case LBM_STORAGE_FP16S: k_interp<Q, LBM_STORAGE_FP16S><<<nb, kIbmThreads, 0, s>>>(a); break;
+      default: k_interp<Q, LBM_STORAGE_BF16S><<<nb, kIbmThreads, 0, s>>>(a); break;
+    }
+    LBM_LAUNCH_CHECK("ibm_interpolate");
+    return LBM_OK;
+  }
+};
+
+static int check_particles(const lbm_particles *pt, const char *who) {
+  if (pt == nullptr || pt->n_particles < 0 || pt->n_markers < 0) {
+    set_error("%s: bad particle description", who);
+    return LBM_ERR_INVALID;
+  }
+  return LBM_OK;
+}
+
+}  // namespace lbm
+
+using namespace lbm;
+
+extern "C" {
+
+int ibm_interpolate(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                    const float *face_rho_in, const float *u_field, const float *rho_field,
+                    const lbm_particles *pt, float dt, int32_t step, uint32_t *status,
+                    void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if ((rc = check_particles(pt, "ibm_interpolate"))) return rc;
+  if (!(dt > 0.f)) {
+    set_error("ibm_interpolate: dt must be positive");
+    return LBM_ERR_INVALID;
+  }
+  if (fa == nullptr && (u_field == nullptr || rho_field == nullptr)) {
+    set_error("ibm_interpolate: needs populations or the u / rho fields");
+    return LBM_ERR_INVALID;
+  }
+  if (fa != nullptr && any_face(lat, LBM_BC_NON_EQUILIBRIUM)) {
+    set_error("ibm_interpolate: NON_EQUILIBRIUM faces need the u / rho fields");
+    return LBM_ERR_UNSUPPORTED;
+  }
+  if (fa != nullptr && any_face(lat, LBM_BC_WALL_WITH_SPEED) && face_rho_in == nullptr) {
+    set_error("ibm_interpolate: WALL_WITH_SPEED faces need face_rho_in");
+    return LBM_ERR_INVALID;
+  }
+  if (pt->n_markers == 0) return LBM_OK;
+  InterpArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = make_geom(lat);
+  a.fa = fa;
+  a.u_field = u_field;
+  a.rho_field = rho_field;
+  if (force != nullptr) {
+    for (int k = 0; k < 3; ++k) a.go[k] = force->old_uniform[k];
+    a.fol_old = force->old_field;
+  }
+  a.face_rho_in = face_rho_in;
+  a.p = *pt;
+  a.dt = dt;
+  a.step = step;
+  a.status = status;
+  switch (lat->q) {
+    case 13: return RunInterp<13>::run(a, lat->storage, (cudaStream_t)stream);
+    case 15: return RunInterp<15>::run(a, lat->storage, (cudaStream_t)stream);
+    case 19: return RunInterp<19>::run(a, lat->storage, (cudaStream_t)stream);
+    default: return RunInterp<27>::run(a, lat->storage, (cudaStream_t)stream);
+  }
+}
+
+int rigid_wall_and_update(const lbm_lattice *lat, const lbm_particles *pt, int32_t what, float dt,
+                          float dx, float gl, float rouf, void *stream) {
+  int rc = LBM_OK;
+  if ((what & RIGID_WALL) && (rc = check_lattice(lat))) return rc;
+  if ((rc = check_particles(pt, "rigid_wall_and_update"))) return rc;
+  if (!(dt > 0.f)) {
+    set_error("Time step must be positive");
+    return LBM_ERR_INVALID;
+  }
+  if (!(rouf > 0.f)) {
+    set_error("Fluid density must be positive");
+    return LBM_ERR_INVALID;
+  }
+  if (pt->n_particles == 0) return LBM_OK;
+  if (what < 1 || what > 3) {
+    set_error("rigid_wall_and_update: what must be RIGID_WALL, RIGID_UPDATE or both");
+    return LBM_ERR_INVALID;
+  }
+  RigidArgs a;
+  a.p = *pt;
+  a.what = what;
+  for (int k = 0; k < 3; ++k) a.size[k] = 0.f;
+  if (lat != nullptr) {
+    a.size[0] = (float)(lat->nx - 1);
+    a.size[1] = (float)(lat->ny - 1);
+    a.size[2] = (float)(lat->nz - 1);
+  }
+  a.dt = dt;
+  a.dx = dx;
+  a.gl = gl;
+  a.rouf = rouf;
+  k_rigid<<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
+  LBM_LAUNCH_CHECK("rigid_wall_and_update");
+  return LBM_OK;
+}
+
+int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
+               uint8_t *chunks, int32_t *owner, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if ((rc = check_particles(pt, "ibm_spread"))) return rc;
+  if (mode != 0 && mode != 1) {
+    set_error("ibm_spread: mode must be 0 (reference) or 1 (accumulate)");
+    return LBM_ERR_INVALID;
+  }
+  if (field == nullptr || chunks == nullptr || (mode == 0 && owner == nullptr)) {
+    set_error("ibm_spread: field, chunks (and owner in reference mode) are required");
+    return LBM_ERR_INVALID;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  SpreadArgs a;
+  a.g = make_geom(lat);
+  a.p = *pt;
+  a.field = field;
+  a.chunks = chunks;
+  a.owner = owner;
+  const long long nchunks = (a.g.n + 31) >> 5;
+  k_spread_clear<<<blocks_for(nchunks * 32, 256), 256, 0, s>>>(a.g.n, field, chunks);
+  LBM_LAUNCH_CHECK("ibm_spread");
+  if (pt->n_markers == 0) return LBM_OK;
+  const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
+  if (mode == 0) {
+    k_spread<0><<<nb, kIbmThreads, 0, s>>>(a);
+    k_spread<1><<<nb, kIbmThreads, 0, s>>>(a);
+    k_spread<2><<<nb, kIbmThreads, 0, s>>>(a);
+  } else {
+    k_spread<3><<<nb, kIbmThreads, 0, s>>>(a);
+  }
+  LBM_LAUNCH_CHECK("ibm_spread");
+  return LBM_OK;
+}
+
+int rigid_update_markers(const lbm_particles *pt, void *stream) {
+  int rc = check_particles(pt, "rigid_update_markers");
+  if (rc) return rc;
+  if (pt->n_particles == 0) return LBM_OK;
+  k_markers<<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
+  LBM_LAUNCH_CHECK("rigid_update_markers");
+  return LBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,349 @@
+// Velocity sets, population storage and the per-node pieces of one LBM step
+// (pull streaming with the reference's face rules, moments, forcing, BGK),
+// shared by every kernel of the library.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <utility>
+
+#include "../../include/funlbm_b200.h"
+
+namespace lbm {
+
+// Compile-time loop: calls fn(std::integral_constant<int, I>) for I < N, so
+// every population index is a constant and f[Q] stays in registers.
+template <typename F, int... I>
+__host__ __device__ __forceinline__ void static_for_impl(F &&fn, std::integer_sequence<int, I...>) {
+  (fn(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__host__ __device__ __forceinline__ void static_for(F &&fn) {
+  static_for_impl(fn, std::make_integer_sequence<int, N>{});
+}
+
+// ---------------------------------------------------------------------------
+// Velocity sets.  Direction order is the reference's (flow/d3/d3q13.py:7-21,
+// d3q15.py:7-23, d3q19.py:8-28, d3q27.py:8-36): the opposite-direction table
+// and the population layout depend on it.  Weights by speed class
+// (d3q13.py:23-39, d3q15.py:25-43, d3q19.py:30-54, d3q27.py:38-71).
+// Tables live inside constexpr functions so that fully unrolled loops fold
+// every lookup to an immediate.
+// ---------------------------------------------------------------------------
+template <int Q>
+struct VSet;
+
+#define LBM_VSET_BODY(QN, EX, EY, EZ, W0, W1, W2, W3)                                   \
+  static constexpr int kQ = QN;                                                           \
+  __host__ __device__ static constexpr int ex(int i) {                                    \
+    constexpr int t[QN] = EX;                                                             \
+    return t[i];                                                                          \
+  }                                                                                       \
+  __host__ __device__ static constexpr int ey(int i) {                                    \
+    constexpr int t[QN] = EY;                                                             \
+    return t[i];                                                                          \
+  }                                                                                       \
+  __host__ __device__ static constexpr int ez(int i) {                                    \
+    constexpr int t[QN] = EZ;                                                             \
+    return t[i];                                                                          \
+  }                                                                                       \
+  __host__ __device__ static constexpr int speed2(int i) {                                \
+    return ex(i) * ex(i) + ey(i) * ey(i) + ez(i) * ez(i);                                \
+  }                                                                                       \
+  __host__ __device__ static constexpr double wd(int i) {                                 \
+    return speed2(i) == 0 ? (W0) : speed2(i) == 1 ? (W1) : speed2(i) == 2 ? (W2) : (W3); \
+  }                                                                                       \
+  __host__ __device__ static constexpr float w(int i) { return (float)wd(i); }           \
+  __host__ __device__ static constexpr int rev(int i) {                                   \
+    int r = 0;                                                                            \
+    for (int j = 0; j < QN; ++j)                                                          \
+      if (ex(j) == -ex(i) && ey(j) == -ey(i) && ez(j) == -ez(i)) r = j;                   \
+    return r;                                                                             \
+  }
+
+#define LBM_ARR(...) {__VA_ARGS__}
+
+template <>
+struct VSet<13> {
+  LBM_VSET_BODY(13,
+                LBM_ARR(0, 1, 1, 1, 1, 0, 0, -1, -1, -1, -1, 0, 0),
+                LBM_ARR(0, 1, -1, 0, 0, 1, 1, -1, 1, 0, 0, -1, -1),
+                LBM_ARR(0, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1),
+                1.0 / 2, 0.0, 1.0 / 24, 0.0)
+};
+template <>
+struct VSet<15> {
+  LBM_VSET_BODY(15,
+                LBM_ARR(0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1),
+                LBM_ARR(0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1),
+                LBM_ARR(0, 0, 0, 0, 0, 1, -1, 1, 1, 1, 1, -1, -1, -1, -1),
+                2.0 / 9, 1.0 / 9, 0.0, 1.0 / 72)
+};
+template <>
+struct VSet<19> {
+  LBM_VSET_BODY(19,
+                LBM_ARR(0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1),
+                LBM_ARR(0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 1, -1, 1, -1, 0, 0, 0, 0),
+                LBM_ARR(0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1),
+                1.0 / 3, 1.0 / 18, 1.0 / 36, 0.0)
+};
+template <>
+struct VSet<27> {
+  LBM_VSET_BODY(27,
+                LBM_ARR(0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, 1, 1, 1,
+                        -1, -1, -1, -1),
+                LBM_ARR(0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1,
+                        1, 1, -1, -1),
+                LBM_ARR(0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1, 1, -1, 1, -1,
+                        1, -1, 1, -1),
+                8.0 / 27, 2.0 / 27, 1.0 / 54, 1.0 / 216)
+};
+
+#undef LBM_ARR
+#undef LBM_VSET_BODY
+
+// ---------------------------------------------------------------------------
+// Population storage.  FP32 stores f; the shifted 16-bit forms store f - w_i
+// (the deviation from the rest-state weight carries all the information and
+// keeps the 16-bit mantissa busy), collided in float32.
+// ---------------------------------------------------------------------------
+template <int S>
+struct Storage;
+
+template <>
+struct Storage<LBM_STORAGE_FP32> {
+  using T = float;
+  __device__ __forceinline__ static float load(const T *p, float) { return __ldg(p); }
+  __device__ __forceinline__ static void store(T *p, float v, float) { *p = v; }
+};
+template <>
+struct Storage<LBM_STORAGE_FP16S> {
+  using T = __half;
+  __device__ __forceinline__ static float load(const T *p, float w) {
+    return w + __half2float(__ldg(p));
+  }
+  __device__ __forceinline__ static void store(T *p, float v, float w) {
+    *p = __float2half_rn(v - w);
+  }
+};
+template <>
+struct Storage<LBM_STORAGE_BF16S> {
+  using T = __nv_bfloat16;
+  __device__ __forceinline__ static float load(const T *p, float w) {
+    return w + __bfloat162float(__ldg(p));
+  }
+  __device__ __forceinline__ static void store(T *p, float v, float w) {
+    *p = __float2bfloat16_rn(v - w);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Lattice constants passed by value to every kernel.
+// ---------------------------------------------------------------------------
+struct Geom {
+  int nx, ny, nz;
+  long long n;      // nodes
+  long long nyz;    // ny * nz
+  int face[LBM_NFACES];
+  float uw[LBM_NFACES][3];
+  long long plane_off[LBM_NFACES];  // offsets of the face-density planes
+  float tau, inv_tau, cs2, inv_cs2, inv_cs4, force_c;  // force_c = 1 - 1/(2 tau)
+  float re_mu;
+  const double *neq_profile;
+};
+
+// face-plane index of node (x, y, z) on face `fc`
+__device__ __forceinline__ long long plane_index(const Geom &g, int fc, int x, int y, int z) {
+  switch (fc >> 1) {
+    case 0: return g.plane_off[fc] + (long long)y * g.nz + z;
+    case 1: return g.plane_off[fc] + (long long)x * g.nz + z;
+    default: return g.plane_off[fc] + (long long)x * g.ny + y;
+  }
+}
+
+__device__ __forceinline__ bool on_any_face(const Geom &g, int x, int y, int z) {
+  return x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1 || z == 0 || z == g.nz - 1;
+}
+
+// ---------------------------------------------------------------------------
+// Pull streaming with the reference's rules (flow/d3/base.py:161-323).
+// For target node t and direction i the reference rolls every population
+// periodically and then overrides, face by face in the order input, output,
+// back, forward, bottom, top, the directions entering through that face; the
+// last matching override wins.  Rolling wraps only where some face override
+// applies, so the source is:
+//   no face applies      -> (t - e_i, i)
+//   PERIODICAL face      -> t with that axis moved to the opposite plane (no
+//                           transverse shift), direction i
+//   WALL face            -> (t, rev(i))                 half-way bounce-back
+//   WALL_WITH_SPEED face -> (t, rev(i)) - 2 rho_t w_i (e_i . uw) / cs^2
+// NON_EQUILIBRIUM x faces are handled by the caller (they need moments).
+// ---------------------------------------------------------------------------
+template <int Q, int S>
+__device__ __forceinline__ void pull_interior(const typename Storage<S>::T *__restrict__ fa,
+                                              const Geom &g, long long idx, float f[Q]) {
+  using V = VSet<Q>;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const long long off = (long long)V::ex(i) * g.nyz + (long long)V::ey(i) * g.nz + V::ez(i);
+    f[i] = Storage<S>::load(fa + (long long)i * g.n + idx - off, V::w(i));
+  });
+}
+
+// Pull population I with face rules.  The governing face is the last one in
+// the order x, y, z whose plane holds the node and through which direction I
+// enters; -1 means none.  `face_rho` is consulted only for WALL_WITH_SPEED
+// faces (density of the previous step at this face node).
+template <int Q, int S, int I>
+__device__ __forceinline__ float pull_one(const typename Storage<S>::T *__restrict__ fa,
+                                          const Geom &g, int x, int y, int z,
+                                          const float *__restrict__ face_rho) {
+  using V = VSet<Q>;
+  constexpr int ex = V::ex(I), ey = V::ey(I), ez = V::ez(I);
+  int fc = -1;
+  if (ex > 0 && x == 0) fc = 0;
+  if (ex < 0 && x == g.nx - 1) fc = 1;
+  if (ey > 0 && y == 0) fc = 2;
+  if (ey < 0 && y == g.ny - 1) fc = 3;
+  if (ez > 0 && z == 0) fc = 4;
+  if (ez < 0 && z == g.nz - 1) fc = 5;
+  int sx = x - ex, sy = y - ey, sz = z - ez, sd = I;
+  float corr = 0.f;
+  if (fc >= 0) {
+    const int code = g.face[fc];
+    sx = x;
+    sy = y;
+    sz = z;
+    if (code == LBM_BC_PERIODICAL) {
+      const int axis = fc >> 1;
+      const bool first = (fc & 1) == 0;
+      if (axis == 0) sx = first ? g.nx - 1 : 0;
+      else if (axis == 1) sy = first ? g.ny - 1 : 0;
+      else sz = first ? g.nz - 1 : 0;
+    } else {
+      sd = V::rev(I);
+      if (code == LBM_BC_WALL_WITH_SPEED) {
+        const float rho_t = face_rho[plane_index(g, fc, x, y, z)];
+        const float eu = (float)ex * g.uw[fc][0] + (float)ey * g.uw[fc][1] + (float)ez * g.uw[fc][2];
+        corr = 2.f * (rho_t * V::w(I)) * eu * g.inv_cs2;
+      }
+    }
+  }
+  const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;
+  const float w_sd = sd == I ? V::w(I) : V::w(V::rev(I));
+  return Storage<S>::load(fa + (long long)sd * g.n + src, w_sd) - corr;
+}
+
+template <int Q, int S, int I = 0>
+struct PullGeneral {
+  __device__ __forceinline__ static void run(const typename Storage<S>::T *__restrict__ fa,
+                                             const Geom &g, int x, int y, int z,
+                                             const float *__restrict__ face_rho, float f[Q]) {
+    f[I] = pull_one<Q, S, I>(fa, g, x, y, z, face_rho);
+    PullGeneral<Q, S, I + 1>::run(fa, g, x, y, z, face_rho, f);
+  }
+};
+template <int Q, int S>
+struct PullGeneral<Q, S, Q> {
+  __device__ __forceinline__ static void run(const typename Storage<S>::T *__restrict__,
+                                             const Geom &, int, int, int,
+                                             const float *__restrict__, float *) {}
+};
+
+template <int Q, int S>
+__device__ __forceinline__ void pull_general(const typename Storage<S>::T *__restrict__ fa,
+                                             const Geom &g, int x, int y, int z,
+                                             const float *__restrict__ face_rho, float f[Q]) {
+  PullGeneral<Q, S>::run(fa, g, x, y, z, face_rho, f);
+}
+
+// Rolled value (periodic wrap on every axis, no face rule): what the
+// reference's f holds at a node before the face overrides run.  Used by the
+// NON_EQUILIBRIUM faces, which read plane 1 / plane X-2 right after the roll.
+template <int Q, int S>
+__device__ __forceinline__ float pull_rolled(const typename Storage<S>::T *__restrict__ fa,
+                                             const Geom &g, int i, int x, int y, int z) {
+  using V = VSet<Q>;
+  int sx = x - V::ex(i), sy = y - V::ey(i), sz = z - V::ez(i);
+  sx = sx < 0 ? sx + g.nx : (sx >= g.nx ? sx - g.nx : sx);
+  sy = sy < 0 ? sy + g.ny : (sy >= g.ny ? sy - g.ny : sy);
+  sz = sz < 0 ? sz + g.nz : (sz >= g.nz ? sz - g.nz : sz);
+  const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;
+  return Storage<S>::load(fa + (long long)i * g.n + src, V::w(i));
+}
+
+// ---------------------------------------------------------------------------
+// Moments (flow/d3/base.py:116-133): rho = sum f, u = (sum f e + F/2) / rho,
+// u := 0 on all six boundary planes whatever their condition.
+// ---------------------------------------------------------------------------
+template <int Q>
+__device__ __forceinline__ void moments(const float f[Q], float fx, float fy, float fz,
+                                        bool face, float &rho, float &ux, float &uy, float &uz) {
+  using V = VSet<Q>;
+  float r = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    r += f[i];
+    if (V::ex(i) > 0) jx += f[i];
+    if (V::ex(i) < 0) jx -= f[i];
+    if (V::ey(i) > 0) jy += f[i];
+    if (V::ey(i) < 0) jy -= f[i];
+    if (V::ez(i) > 0) jz += f[i];
+    if (V::ez(i) < 0) jz -= f[i];
+  });
+  rho = r;
+  const float inv = 1.f / r;
+  ux = face ? 0.f : (jx + 0.5f * fx) * inv;
+  uy = face ? 0.f : (jy + 0.5f * fy) * inv;
+  uz = face ? 0.f : (jz + 0.5f * fz) * inv;
+}
+
+// Forcing term of FlowD3.cul_equ2 (flow/d3/base.py:103-114):
+//   f_i += (1 - 1/(2 tau)) w_i [ (e_i - u)/cs^2 + (u o e_i) o e_i / cs^4 ] . F
+// (component-wise u_k e_ik^2, the reference's form).
+template <int Q>
+__device__ __forceinline__ void add_force(float f[Q], const Geom &g, float ux, float uy, float uz,
+                                          float fx, float fy, float fz) {
+  using V = VSet<Q>;
+  const float uF = ux * fx + uy * fy + uz * fz;
+  const float ax = ux * fx, ay = uy * fy, az = uz * fz;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const float eF = (float)V::ex(i) * fx + (float)V::ey(i) * fy + (float)V::ez(i) * fz;
+    const float t2 = (V::ex(i) ? ax : 0.f) + (V::ey(i) ? ay : 0.f) + (V::ez(i) ? az : 0.f);
+    f[i] += g.force_c * V::w(i) * ((eF - uF) * g.inv_cs2 + t2 * g.inv_cs4);
+  });
+}
+
+// BGK collision of FlowD3.cul_equ (flow/d3/base.py:150-159):
+//   feq_i = (1 + t + t^2/2 - |u|^2/(2 cs^2)) rho w_i,  t = e_i.u / cs^2
+//   f_i  <- f_i - (f_i - feq_i) / tau
+template <int Q>
+__device__ __forceinline__ float feq_of(const Geom &g, int i, float rho, float ux, float uy,
+                                        float uz, float u2) {
+  using V = VSet<Q>;
+  const float t = ((float)V::ex(i) * ux + (float)V::ey(i) * uy + (float)V::ez(i) * uz) * g.inv_cs2;
+  return (1.f + t + 0.5f * t * t - u2) * (rho * V::w(i));
+}
+
+template <int Q>
+__device__ __forceinline__ void collide(float f[Q], const Geom &g, float rho, float ux, float uy,
+                                        float uz) {
+  const float u2 = (ux * ux + uy * uy + uz * uz) * 0.5f * g.inv_cs2;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const float feq = feq_of<Q>(g, i, rho, ux, uy, uz, u2);
+    f[i] = f[i] - (f[i] - feq) * g.inv_tau;
+  });
+}
+
+__device__ __forceinline__ void flag_bad(unsigned *status, float rho, float ux, float uy, float uz) {
+  if (status == nullptr) return;
+  if (!(rho > 0.f) || !(rho < 3.0e38f)) atomicOr(status, LBM_STATUS_RHO_BAD);
+  if (!(fabsf(ux) + fabsf(uy) + fabsf(uz) < 3.0e38f)) atomicOr(status, LBM_STATUS_U_BAD);
+}
+
+}  // namespace lbm

@@ -1,0 +1,220 @@
+/*
+ * funlbm_b200 -- C ABI of the B200 (sm_100a) lattice-Boltzmann step path.
+ *
+ * Every entry point replaces one function (or a fused sequence of functions)
+ * of funlbm 1.2.0; the reference function is cited beside each declaration as
+ * file:line inside the funlbm source tree (src/funlbm/...).
+ *
+ * Conventions
+ *  - All buffers are device pointers allocated and owned by the caller; the
+ *    library never allocates or frees them.  Sizes are element counts.
+ *  - Populations are stored structure-of-arrays, f[q][x][y][z] (z fastest),
+ *    in the storage type named by lbm_lattice.storage.  Node counts are the
+ *    reference's size + 1 per axis.  Velocity, force: [x][y][z][3] float32;
+ *    density: [x][y][z] float32 -- the reference's own [X,Y,Z,3] / [X,Y,Z,1].
+ *  - `stream` is a cudaStream_t (NULL = the legacy default stream).  Calls are
+ *    asynchronous on that stream; results are ready when the stream is.
+ *  - Every call returns LBM_OK (0) or an error code; lbm_last_error() returns a
+ *    message for the calling thread.  Nothing is thrown across the ABI.
+ *  - Calls on different lattices are independent.  Calls on one lattice must
+ *    be ordered by the caller (same stream, or events).
+ */
+#ifndef FUNLBM_B200_H
+#define FUNLBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define LBM_OK 0
+#define LBM_ERR_INVALID 1     /* bad argument: the reference raises ValueError   */
+#define LBM_ERR_UNSUPPORTED 2 /* face code / velocity set: NotImplementedError   */
+#define LBM_ERR_CUDA 3        /* CUDA launch or runtime error                    */
+
+/* ---- device status word bits (written by kernels with atomicOr) --------- */
+#define LBM_STATUS_RHO_BAD 0x1u      /* density <= 0 or not finite at some node  */
+#define LBM_STATUS_U_BAD 0x2u        /* velocity not finite at some node         */
+#define LBM_STATUS_STENCIL_EMPTY 0x4u /* a marker's normalised weight sum != 1   */
+                                      /* after step 100 (lbm/lbm3d.py:84-86)     */
+
+/* ---- boundary codes: values of funlbm's BoundaryCondition (config/base.py:17-23) */
+#define LBM_BC_PERIODICAL 11000
+#define LBM_BC_WALL 1200
+#define LBM_BC_WALL_WITH_SPEED 1201
+#define LBM_BC_NON_EQUILIBRIUM 1400
+
+/* face order: input (x=0), output (x=X-1), back (y=0), forward (y=Y-1),
+ * bottom (z=0), top (z=Z-1) -- the order of FlowD3.f_stream_bound
+ * (flow/d3/base.py:183-196); a later face overrides an earlier one. */
+#define LBM_NFACES 6
+
+/* ---- population storage ------------------------------------------------ */
+#define LBM_STORAGE_FP32 0  /* float32 populations (the reference's type)       */
+#define LBM_STORAGE_FP16S 1 /* float16 of (f_i - w_i), collided in float32       */
+#define LBM_STORAGE_BF16S 2 /* bfloat16 of (f_i - w_i), collided in float32      */
+
+/* One lattice: velocity set, shape, faces and relaxation.  Mirrors the
+ * reference's FlowConfig + Param (flow/base.py:15-114, flow/d3/base.py:72-101). */
+typedef struct lbm_lattice {
+  int32_t q;              /* 13, 15, 19 or 27 (create_flow, flow/__init__.py:16-41) */
+  int32_t nx, ny, nz;     /* node counts = size + 1 (flow/d3/base.py:81-82)         */
+  int32_t face[LBM_NFACES];        /* LBM_BC_* per face                             */
+  float face_uw[LBM_NFACES][3];    /* wall velocity of WALL_WITH_SPEED faces         */
+  float tau;              /* float32(3 mu + 0.5) (flow/d3/base.py:96)               */
+  float cs2;              /* float32(sqrt(1/3))^2 (flow/base.py:37-39)              */
+  int32_t storage;        /* LBM_STORAGE_*                                          */
+  float re_mu;            /* Re * mu, NON_EQUILIBRIUM inlet scale (flow/d3/base.py:137-143) */
+  const double *neq_profile; /* device [ny*nz] duct profile init_u / u_max (float64, */
+                             /* as cul_u returns it); NULL unless face[0] is NEQ    */
+} lbm_lattice;
+
+/* Forcing seen by one step: FOL = uniform + field.  `uniform` is a body force
+ * applied at every node; `field` is the spread IBM force ([x][y][z][3], zero
+ * outside the 32-node chunks flagged in `chunks`; NULL = no field).
+ * "old" is the FOL of the previous step (used by the first moment pass,
+ * update_u_rou after f_stream, lbm/base.py:159-163); "new" the FOL of this
+ * step (cul_equ2 and the second update_u_rou, lbm/base.py:173-175). */
+typedef struct lbm_force {
+  float old_uniform[3];
+  float new_uniform[3];
+  const float *old_field;
+  const float *new_field;
+  const uint8_t *old_chunks; /* [ceil(n/32)] flags, NULL = all chunks */
+  const uint8_t *new_chunks;
+} lbm_force;
+
+/* Optional per-step outputs: the reference's state at the end of the step
+ * (flow.f after cul_equ2, rou / u after the second update_u_rou). */
+typedef struct lbm_observe {
+  float *f;   /* float32 SoA [q][x][y][z] or NULL */
+  float *rho; /* [x][y][z] or NULL */
+  float *u;   /* [x][y][z][3] or NULL */
+} lbm_observe;
+
+/* Bytes of the caller-allocated face-density plane buffer for a lattice
+ * (2*ny*nz + 2*nx*nz + 2*nx*ny floats; needed when a face is WALL_WITH_SPEED
+ * or NON_EQUILIBRIUM, else may be NULL). */
+size_t lbm_face_plane_floats(const lbm_lattice *lat);
+
+/* Validate a lattice description.  Returns LBM_ERR_UNSUPPORTED for a face code
+ * the reference cannot stream (flow/d3/base.py:218-219, 242-243, 262-263, ...)
+ * and LBM_ERR_INVALID for a bad shape, velocity set or tau. */
+int lbm_lattice_check(const lbm_lattice *lat);
+
+/* FlowD3.init + the first LBMD3._init collision (flow/d3/base.py:72-101,
+ * lbm/lbm3d.py:23-27), followed by step 1's collision, which the reference
+ * applies with the init-time moments: writes post-collision populations
+ * `fa` (storage type).  `f0` is an optional float32 SoA initial field
+ * (NULL = rho*w with rho = 1).  `face_rho` receives the density on the six
+ * face planes (may be NULL when no face needs it). */
+int lbm_flow_init(const lbm_lattice *lat, const float *f0, void *fa, float *face_rho,
+                  void *stream);
+
+/* One fused time step: f_stream + update_u_rou + cul_equ2 + update_u_rou of
+ * step k and the cul_equ of step k+1 (lbm/base.py:159-175,
+ * flow/d3/base.py:103-181) in one sweep.  Reads post-collision populations
+ * `fa`, writes post-collision populations `fb` (fb may be NULL: observation
+ * only, nothing but `obs` is written).  face_rho_in / face_rho_out hold the
+ * face-plane densities before / after the step (WALL_WITH_SPEED, NEQ).
+ * `status` (may be NULL) receives LBM_STATUS_* bits. */
+int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
+                  const float *face_rho_in, float *face_rho_out, const lbm_observe *obs,
+                  uint32_t *status, void *stream);
+
+/* Single reference functions on float32 SoA populations, for callers that
+ * invoke FlowD3's methods one at a time. */
+/* FlowD3.cul_equ (flow/d3/base.py:150-159): f <- f - (f - feq)/tau in place;
+ * feq (may be NULL) receives the equilibrium. */
+int lbm_collide(const lbm_lattice *lat, float *f, const float *rho, const float *u, float *feq,
+                void *stream);
+/* FlowD3.f_stream + f_stream_bound* (flow/d3/base.py:161-323): f_out from
+ * f_in (the reference's fcopy).  rho: densities for WALL_WITH_SPEED faces;
+ * feq: equilibrium of the last cul_equ for NON_EQUILIBRIUM faces. */
+int lbm_stream(const lbm_lattice *lat, const float *f_in, float *f_out, const float *rho,
+               const float *feq, void *stream);
+/* FlowD3.update_u_rou + update_u_rou_boundary (flow/d3/base.py:116-148):
+ * rho, u, p from f and FOL (fol may be NULL = zero).  `scratch` is one
+ * caller-allocated float used for the inlet's global density maximum when
+ * the input face is NON_EQUILIBRIUM (else may be NULL). */
+int lbm_moments(const lbm_lattice *lat, const float *f, const float *fol, float *rho, float *u,
+                float *p, float *scratch, void *stream);
+/* FlowD3.cul_equ2 (flow/d3/base.py:103-114): f += forcing(u, FOL) in place. */
+int lbm_add_force(const lbm_lattice *lat, float *f, const float *u, const float *fol,
+                  void *stream);
+
+/* ---- immersed boundary and rigid particles ------------------------------ */
+
+/* Marker / particle state of all particles of one lattice, concatenated in
+ * the reference's (particle, marker) loop order.  Float32 like the reference,
+ * except the particle state that is integrated in float64. */
+typedef struct lbm_particles {
+  int32_t n_particles;
+  int32_t n_markers;             /* total over all particles                  */
+  const int32_t *marker_offset;  /* [n_particles + 1] first marker of each    */
+  const int32_t *marker_owner;   /* [n_markers] particle index of each marker */
+  const float *lagrange;         /* [n_markers][3] body-frame marker points   */
+  float *lx;                     /* [n_markers][3] marker positions           */
+  float *lu;                     /* [n_markers][3] rigid velocity at markers  */
+  float *lF;                     /* [n_markers][3] marker force               */
+  float *lrou;                   /* [n_markers] interpolated density          */
+  const float *lm;               /* [n_markers] marker area weight            */
+  float *cx, *cu, *cw, *cF, *cT; /* [n_particles][3] float32 mirrors          */
+  float *angle;                  /* [n_particles][3] rotation vector          */
+  const float *mass;             /* [n_particles]                             */
+  const float *inertia;          /* [n_particles][3]                          */
+  const float *rou;              /* [n_particles] particle density            */
+} lbm_particles;
+
+/* LBMD3.flow_to_lagrange (lbm/lbm3d.py:66-100) fused with the moment pass
+ * it reads: for every marker, streams the 4x4x4 stencil nodes from the
+ * post-collision populations `fa`, takes the first update_u_rou moments there
+ * (with the previous step's force), interpolates with the normalised cosine
+ * delta, and writes lu (rigid velocity), lF and lrou.  With fa == NULL the
+ * moments are read from `u_field` ([x][y][z][3]) and `rho_field` ([x][y][z])
+ * instead (the reference's flow.u / flow.rou).  `step` is the reference's
+ * step counter (the weight-sum sentinel is active after step 100). */
+int ibm_interpolate(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                    const float *face_rho_in, const float *u_field, const float *rho_field,
+                    const lbm_particles *pt, float dt, int32_t step, uint32_t *status,
+                    void *stream);
+
+/* LBMD3.particle_to_wall (lbm/lbm3d.py:121-167) and
+ * Particle.update_from_lar (particle/base/base.py:120-151) for all particles:
+ * the spring force on the six extreme markers (what & 1), then force / torque
+ * sums over markers in float64 and the explicit Euler update of cu, cx, cw
+ * (what & 2).  `lat` (the wall bounds) may be NULL when what == RIGID_UPDATE. */
+#define RIGID_WALL 1
+#define RIGID_UPDATE 2
+int rigid_wall_and_update(const lbm_lattice *lat, const lbm_particles *pt, int32_t what, float dt,
+                          float dx, float gl, float rouf, void *stream);
+
+/* LBMD3.lagrange_to_flow (lbm/lbm3d.py:102-119): FOL := 0, then each
+ * marker's stencil box receives w * lF * lm.  mode 0 = the reference's
+ * assignment, the last (particle, marker) in loop order wins; mode 1 =
+ * accumulation (the physical spreading sum).  `field` is [x][y][z][3];
+ * `chunks` flags the 32-node chunks written (and, on entry, those written
+ * last time, which are cleared first); `owner` is an int32 scratch array of
+ * n nodes that must hold -1 everywhere on entry and holds -1 again on exit. */
+int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
+               uint8_t *chunks, int32_t *owner, void *stream);
+
+/* Particle.update + Coordinate.update/cul_point (particle/base/base.py:153-156,
+ * particle/coord.py:87-108): angle += cw; lx = R(angle) lagrange + cx, with the
+ * rotation built in float64 from the rotation vector. */
+int rigid_update_markers(const lbm_particles *pt, void *stream);
+
+/* Thread-local message of the last failed call. */
+const char *lbm_last_error(void);
+
+/* Library version string. */
+const char *lbm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FUNLBM_B200_H */

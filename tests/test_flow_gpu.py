@@ -1,0 +1,291 @@
+"""GPU parity of the flow path (C ABI through funlbm_b200) against the
+reference's golden vectors and the oracle.
+
+Tolerances (float32 throughout, as the reference):
+  * single functions vs reference golden: max relative error <= 2e-6;
+  * multi-step f, rho: max relative error <= 1e-5; u: max abs error
+    <= 1e-5 * max|u| + 2e-7 (u is a small difference of O(1) sums, so its
+    float32 noise is absolute, ~3e-8 per step);
+  * 1000 steps: max relative error <= 1e-5 in rho and in u (u normalised by
+    max|u|), the bound stated for particle-free cases.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lbm_oracle as O
+from tests.gpu_util import (init_with, lbm_config, rel_err, require_cuda, run, smooth_f0, to_np)
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    require_cuda()
+
+
+def _flow(q, size, mu, codes, uw=None, Re=10.0):
+    from funlbm_b200.flow import create_flow
+    from tests.gpu_util import boundary_json
+    from funlbm_b200.flow import FlowConfig
+
+    cfg = FlowConfig().from_json({"size": list(size), "param_type": "D3Q%d" % q,
+                                  "param": {"mu": mu, "Re": Re},
+                                  "boundary": boundary_json(codes, uw)})
+    fl = create_flow(cfg, device="cuda")
+    fl.init()
+    return fl
+
+
+def _t(a):
+    return torch.tensor(a, device="cuda")
+
+
+@pytest.mark.parametrize("q", [13, 15, 19, 27])
+def test_single_functions_vs_reference(q):
+    """cul_equ / f_stream / update_u_rou / cul_equ2, one kernel each, on the
+    reference's own random states and face mixes (incl. WALL_WITH_SPEED and
+    NON_EQUILIBRIUM)."""
+    g = np.load(os.path.join(GOLD, "kat_q%d.npz" % q))
+    for c in range(int(g["ncase"])):
+        p = "c%d_" % c
+        fl = _flow(q, (4, 5, 6), float(g[p + "mu"]), g[p + "faces"], g[p + "uw"], float(g[p + "Re"]))
+        fl.f, fl.u, fl.rou, fl.FOL = (_t(g[p + k]) for k in ("f", "u", "rou", "FOL"))
+        fl.cul_equ()
+        assert rel_err(to_np(fl.f), g[p + "collide_f"]) < 2e-6
+        assert rel_err(to_np(fl.feq), g[p + "collide_feq"]) < 2e-6
+        fl.f = _t(g[p + "f"])
+        fl.f_stream()
+        assert rel_err(to_np(fl.f), g[p + "stream_f"]) < 2e-6, (c, g[p + "faces"])
+        fl.FOL = _t(g[p + "FOL"])
+        fl.update_u_rou()
+        assert rel_err(to_np(fl.rou), g[p + "moments_rou"]) < 2e-6
+        assert rel_err(to_np(fl.u), g[p + "moments_u"]) < 2e-6
+        assert rel_err(to_np(fl.p), g[p + "moments_p"]) < 2e-6
+        fl.f, fl.u, fl.FOL = _t(g[p + "f"]), _t(g[p + "u"]), _t(g[p + "FOL"])
+        fl.cul_equ2()
+        assert rel_err(to_np(fl.f), g[p + "force_f"]) < 2e-6
+
+
+def _check_state(lbm, ref_f, ref_u, ref_rou):
+    f, u, rou = to_np(lbm.flow.f), to_np(lbm.flow.u), to_np(lbm.flow.rou)
+    assert rel_err(f, ref_f) < 1e-5
+    assert rel_err(rou, ref_rou) < 1e-5
+    assert np.abs(u - ref_u).max() <= 1e-5 * np.abs(ref_u).max() + 2e-7
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("fused", [True, False])
+def test_run_step_vs_reference(q, fused):
+    """LBMD3.run_step sequences recorded from the reference (12 steps,
+    PERIODICAL/WALL mixes), fused path and reference call sequence."""
+    from funlbm_b200.lbm import LBMD3
+
+    g = np.load(os.path.join(GOLD, "steps_q%d.npz" % q))
+    for c in range(int(g["ncase"])):
+        p = "c%d_" % c
+        lbm = LBMD3(config=lbm_config(q, tuple(g["size"]), float(g[p + "mu"]), g[p + "faces"],
+                                      fused=fused))
+        init_with(lbm, g[p + "f0"])
+        run(lbm, int(g["nsteps"]))
+        _check_state(lbm, g[p + "f"], g[p + "u"], g[p + "rou"])
+
+
+def _oracle_run(q, size, mu, codes, uw, f0, nsteps, body_force=None, dtype=np.float32):
+    faces = dict(zip(O.FACES, [int(c) for c in codes]))
+    uwd = None if uw is None else {k: uw[i] for i, k in enumerate(O.FACES)}
+    fl = O.OracleFlow(q, size, mu, faces, uwd, dtype=dtype)
+    lbm = O.OracleLBM(fl, body_force=body_force)
+    lbm.init(f0)
+    lbm.run(nsteps)
+    return fl
+
+
+@pytest.mark.parametrize("q", [13, 15, 19, 27])
+def test_fused_random_faces_vs_oracle(q):
+    """Random PERIODICAL / WALL / WALL_WITH_SPEED mixes, with and without a
+    body force, ragged shapes, 25 steps."""
+    from funlbm_b200.lbm import LBMD3
+
+    rng = np.random.default_rng(q)
+    for case in range(3):
+        size = tuple(int(v) for v in rng.integers(4, 11, 3))
+        shape = tuple(s + 1 for s in size)
+        codes = rng.choice([11000, 1200, 1201], 6)
+        uw = (0.02 * rng.standard_normal((6, 3))).astype(np.float32)
+        bf = None if case == 0 else (1e-5 * rng.standard_normal(3)).tolist()
+        mu = float(rng.uniform(0.03, 0.2))
+        f0 = smooth_f0(q, shape, 0.04, 10 * q + case)
+        lbm = LBMD3(config=lbm_config(q, size, mu, codes, uw, body_force=bf))
+        init_with(lbm, f0)
+        run(lbm, 25)
+        ref = _oracle_run(q, size, mu, codes, uw, f0, 25, body_force=bf)
+        _check_state(lbm, ref.f, ref.u, ref.rou)
+
+
+def test_fused_equals_reference_sequence():
+    """The fused kernel and the one-kernel-per-function sequence give the same
+    state (only float32 rounding order differs)."""
+    from funlbm_b200.lbm import LBMD3
+
+    q, size = 19, (23, 17, 29)
+    codes = [1200, 1200, 11000, 11000, 1201, 1200]
+    uw = np.zeros((6, 3), np.float32)
+    uw[4] = (0.01, -0.02, 0.0)
+    f0 = smooth_f0(q, tuple(s + 1 for s in size), 0.05, 3)
+    out = []
+    for fused in (True, False):
+        lbm = LBMD3(config=lbm_config(q, size, 0.07, codes, uw, body_force=[1e-5, 0, -2e-5],
+                                      fused=fused))
+        init_with(lbm, f0)
+        run(lbm, 30)
+        out.append((to_np(lbm.flow.f), to_np(lbm.flow.u), to_np(lbm.flow.rou)))
+    assert rel_err(out[0][0], out[1][0]) < 2e-6
+    assert rel_err(out[0][2], out[1][2]) < 2e-6
+    assert np.abs(out[0][1] - out[1][1]).max() < 1e-6 * np.abs(out[1][1]).max() + 1e-7
+
+
+def test_1000_steps_vs_oracle():
+    """The particle-free bound: <= 1e-5 relative in rho and u after 1000
+    float32 steps (u normalised by max|u|)."""
+    from funlbm_b200.lbm import LBMD3
+
+    q, size = 19, (15, 11, 9)
+    codes = [1200, 1200, 11000, 11000, 1200, 1200]
+    f0 = smooth_f0(q, tuple(s + 1 for s in size), 0.05, 1000)
+    lbm = LBMD3(config=lbm_config(q, size, 0.1, codes, body_force=[2e-6, 0, 1e-6]))
+    init_with(lbm, f0)
+    run(lbm, 1000)
+    ref = _oracle_run(q, size, 0.1, codes, None, f0, 1000, body_force=[2e-6, 0, 1e-6])
+    u, rou = to_np(lbm.flow.u), to_np(lbm.flow.rou)
+    assert rel_err(rou, ref.rou) <= 1e-5
+    assert np.abs(u - ref.u).max() / np.abs(ref.u).max() <= 1e-5
+
+
+def test_c_abi_direct_init_and_step():
+    """Lattice (raw C ABI): lbm_flow_init with an initial field, fused steps,
+    observation -- against the oracle."""
+    from funlbm_b200.lattice import Lattice, cs2_float32, make_force, tau_float32
+
+    q, size = 27, (12, 9, 14)
+    shape = tuple(s + 1 for s in size)
+    codes = [11000, 11000, 1200, 1201, 11000, 11000]
+    uw = np.zeros((6, 3), np.float32)
+    uw[3] = (0.03, 0.0, -0.01)
+    mu = 0.09
+    f0 = smooth_f0(q, shape, 0.04, 77)
+    lat = Lattice(q, shape, codes, tau_float32(mu), face_uw=uw.tolist(), device="cuda")
+    f0_soa = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda")
+    lat.init(f0_soa)
+    force = make_force((0, 0, 0), (0, 0, 0))
+    for _ in range(10):
+        lat.step(force)
+    f = torch.empty(q * lat.n, device="cuda")
+    rho = torch.empty(lat.n, device="cuda")
+    u = torch.empty(lat.n * 3, device="cuda")
+    lat.observe(force, f=f, rho=rho, u=u)
+    torch.cuda.synchronize()
+    ref = _oracle_run(q, size, mu, codes, uw, f0, 10)
+    f_ref = np.moveaxis(ref.f, -1, 0).reshape(q, -1)
+    assert rel_err(to_np(f).reshape(q, -1), f_ref) < 1e-5
+    assert rel_err(to_np(rho), ref.rou.reshape(-1)) < 1e-5
+    assert np.abs(to_np(u) - ref.u.reshape(-1)).max() <= 1e-5 * np.abs(ref.u).max() + 2e-7
+    assert lat.read_status() == 0
+    assert abs(cs2_float32() - float(ref.cs2)) == 0.0
+
+
+def test_periodic_mass_conservation_large():
+    """128^3 periodic cube: total mass is conserved to float32 rounding, and the
+    velocity field of a Taylor-Green vortex stays finite and decays."""
+    from funlbm_b200.lbm import LBMD3
+
+    q, size = 19, (127, 127, 127)
+    lbm = LBMD3(config=lbm_config(q, size, 1.0 / 30, [11000] * 6))
+    lbm.config.flow_config.init_field = {"type": "taylor_green", "u0": 0.05}
+    lbm.init()
+    m0 = float(lbm.flow.rou.double().sum())
+    ke0 = float((lbm.flow.u.double() ** 2).sum())
+    run(lbm, 50)
+    m1 = float(lbm.flow.rou.double().sum())
+    ke1 = float((lbm.flow.u.double() ** 2).sum())
+    assert abs(m1 - m0) / m0 < 1e-5
+    assert 0 < ke1 < ke0
+    assert lbm.check_status() == 0
+
+
+def test_status_word_flags_bad_density():
+    """A NaN population sets LBM_STATUS_RHO_BAD in the device status word; the
+    context stays usable."""
+    from funlbm_b200 import _lib
+    from funlbm_b200.lbm import LBMD3
+
+    q, size = 19, (7, 7, 7)
+    f0 = smooth_f0(q, tuple(s + 1 for s in size), 0.02, 5)
+    f0[3, 3, 3, 5] = np.nan
+    lbm = LBMD3(config=lbm_config(q, size, 0.1, [11000] * 6))
+    init_with(lbm, f0)
+    run(lbm, 2)
+    word = lbm.check_status()
+    assert word & _lib.LBM_STATUS_RHO_BAD
+    assert lbm.run_status is False
+    lbm2 = LBMD3(config=lbm_config(q, size, 0.1, [11000] * 6))
+    init_with(lbm2, smooth_f0(q, tuple(s + 1 for s in size), 0.02, 6))
+    run(lbm2, 2)
+    assert lbm2.check_status() == 0
+
+
+def taylor_green_f0(q, shape, u0):
+    """f = feq(rho = 1, u_TG) in float32 with the reference's feq formula
+    (flow/d3/base.py:152-158); u_TG = u0 (sin kx cos ky cos kz,
+    -cos kx sin ky cos kz, 0), k = 2 pi / N per axis."""
+    e, w, _ = O.velocity_set(q)
+    X, Y, Z = shape
+    x = np.arange(X)[:, None, None] * (2 * np.pi / X)
+    y = np.arange(Y)[None, :, None] * (2 * np.pi / Y)
+    z = np.arange(Z)[None, None, :] * (2 * np.pi / Z)
+    ux = u0 * np.sin(x) * np.cos(y) * np.cos(z)
+    uy = -u0 * np.cos(x) * np.sin(y) * np.cos(z)
+    u = np.stack(np.broadcast_arrays(ux, uy, 0 * ux), -1).astype(np.float32)
+    cs2 = O.cs2_of(np.float32)
+    tmp = (u @ e.T.astype(np.float32)) / cs2
+    u2 = np.sqrt((u * u).sum(-1, keepdims=True)) ** 2 / cs2 / np.float32(2)
+    return ((1 + tmp + tmp ** 2 / 2 - u2) * w.astype(np.float32)).astype(np.float32)
+
+
+def test_init_field_taylor_green():
+    """The init_field extension sets f = feq(1, u_TG) after FlowD3.init."""
+    from funlbm_b200.flow import FlowConfig, create_flow
+
+    cfg = FlowConfig().from_json({"size": [15, 11, 7], "param_type": "D3Q19",
+                                  "init_field": {"type": "taylor_green", "u0": 0.05}})
+    fl = create_flow(cfg, device="cuda")
+    fl.init()
+    ref = taylor_green_f0(19, (16, 12, 8), 0.05)
+    assert rel_err(to_np(fl.f), ref) < 1e-6
+
+
+@pytest.mark.parametrize("storage,bound", [("fp16s", 1e-3), ("bf16s", 2e-2)])
+def test_shifted_storage_vs_fp64(storage, bound):
+    """FP16 / BF16 deviations from w, collided in float32, against an FP64
+    oracle run of the same Taylor-Green case (48^3 periodic, 200 steps).
+    Errors: rho relative, u normalised by max|u|."""
+    from funlbm_b200.lbm import LBMD3
+
+    q, size = 19, (47, 47, 47)
+    shape = tuple(s + 1 for s in size)
+    f0 = taylor_green_f0(q, shape, 0.05)
+    lbm = LBMD3(config=lbm_config(q, size, 1.0 / 30, [11000] * 6, storage=storage))
+    init_with(lbm, f0)
+    run(lbm, 200)
+    ref = _oracle_run(q, size, 1.0 / 30, [11000] * 6, None, f0.astype(np.float64), 200,
+                      dtype=np.float64)
+    u, rou = to_np(lbm.flow.u), to_np(lbm.flow.rou)
+    e_rho = rel_err(rou, ref.rou)
+    e_u = np.abs(u - ref.u).max() / np.abs(ref.u).max()
+    print("%s: rho err %.2e, u err %.2e" % (storage, e_rho, e_u))
+    assert e_rho <= bound and e_u <= bound
