@@ -152,19 +152,30 @@ def test_fused_equals_reference_sequence():
 
 def test_1000_steps_vs_oracle():
     """The particle-free bound: <= 1e-5 relative in rho and u after 1000
-    float32 steps (u normalised by max|u|)."""
+    float32 steps (u normalised by max|u|).  A lid-driven cavity (top face
+    WALL_WITH_SPEED, uw = (0.05, 0, 0)) keeps |u| ~ 1.5e-2; undriven cases
+    decay to |u| ~ 1e-6 (the reference zeroes u on all six planes), where any
+    two float32 implementations differ by more than 1e-5 relative.  For this
+    case the float32 oracle itself differs from a float64 run by 6e-6 (u) and
+    8e-6 (rho)."""
     from funlbm_b200.lbm import LBMD3
 
     q, size = 19, (15, 11, 9)
-    codes = [1200, 1200, 11000, 11000, 1200, 1200]
-    f0 = smooth_f0(q, tuple(s + 1 for s in size), 0.05, 1000)
-    lbm = LBMD3(config=lbm_config(q, size, 0.1, codes, body_force=[2e-6, 0, 1e-6]))
+    codes = [1200, 1200, 1200, 1200, 1200, 1201]
+    uw = np.zeros((6, 3), np.float32)
+    uw[5] = (0.05, 0.0, 0.0)
+    f0 = smooth_f0(q, tuple(s + 1 for s in size), 0.01, 1000)
+    lbm = LBMD3(config=lbm_config(q, size, 0.1, codes, uw))
     init_with(lbm, f0)
     run(lbm, 1000)
-    ref = _oracle_run(q, size, 0.1, codes, None, f0, 1000, body_force=[2e-6, 0, 1e-6])
+    ref = _oracle_run(q, size, 0.1, codes, uw, f0, 1000)
     u, rou = to_np(lbm.flow.u), to_np(lbm.flow.rou)
-    assert rel_err(rou, ref.rou) <= 1e-5
-    assert np.abs(u - ref.u).max() / np.abs(ref.u).max() <= 1e-5
+    e_rho = rel_err(rou, ref.rou)
+    e_u = np.abs(u - ref.u).max() / np.abs(ref.u).max()
+    print("1000 steps: rho rel err %.2e, u rel err %.2e, max|u| %.3g" % (e_rho, e_u, np.abs(ref.u).max()))
+    assert np.abs(ref.u).max() > 1e-2
+    assert e_rho <= 1e-5
+    assert e_u <= 1e-5
 
 
 def test_c_abi_direct_init_and_step():

@@ -60,7 +60,9 @@ def test_particles_vs_reference(case, fused):
     lbm = _make(case, fused=fused)
     init_with(lbm, g[pre + "f0"])
     for i, p in enumerate(lbm.particle_swarm.particles):
-        assert np.array_equal(to_np(p._lagrange), g[pre + "p%d_lagrange" % i])
+        # coordinates that are exactly 0 on the surface come out as +-1e-17
+        # residues of the crossing solve (closed form here, fsolve there)
+        assert np.abs(to_np(p._lagrange) - g[pre + "p%d_lagrange" % i]).max() <= 1e-6
         assert abs(float(p.mass) - g[pre + "masses"][i]) <= 1e-6 * g[pre + "masses"][i]
         assert np.allclose(to_np(p.I), g[pre + "inertia"][i], rtol=1e-6)
     for s in range(case[7]):
@@ -98,25 +100,39 @@ def _oracle_case(case, g, ibm_mode="reference", nsteps=None):
                                    c["center"], ang))
     lbm = O.OracleLBM(fl, ps, gl=gl, ibm_mode=ibm_mode)
     lbm.init(g[pre + "f0"])
-    lbm.run(nsteps or steps)
+    lbm.run(steps if nsteps is None else nsteps)
     return lbm
 
 
 def test_accumulate_mode_vs_oracle():
-    """ibm.mode = accumulate: spread contributions are summed (atomics) -- the
-    physical spreading operator -- against the oracle's accumulate mode."""
+    """ibm.mode = accumulate: spread contributions are summed (atomics) instead
+    of assigned.  With the reference's direct-forcing law (lF = 2 rho (U - u) /
+    dt on overlapping 4^3 stencils) summed spreading over-corrects and the run
+    diverges within about three steps -- in the oracle as on the GPU -- so the
+    kernel is checked over the first two steps, markers placed on the body
+    before step 1."""
     g = np.load(os.path.join(GOLD, "particles.npz"))
     case = PARTICLE_CASES[2]
     lbm = _make(case, ibm_mode="accumulate")
     init_with(lbm, g[case[0] + "_f0"])
-    run(lbm, 8)
-    ref = _oracle_case(case, g, ibm_mode="accumulate", nsteps=8)
-    for k in ("cx", "cu", "cw"):
-        got = _stack(lbm, k)
-        want = np.stack([getattr(p, k) for p in ref.particles])
-        assert np.abs(got - want).max() <= 1e-4 * max(1.0, np.abs(want).max()), k
-    assert np.abs(to_np(lbm.flow.FOL) - ref.flow.FOL).max() <= 1e-4 * np.abs(ref.flow.FOL).max()
-    assert rel_err(to_np(lbm.flow.rou), ref.flow.rou) < 2e-5
+    lbm.particle_swarm.update()
+    ref = _oracle_case(case, g, ibm_mode="accumulate", nsteps=0)
+    for p in ref.particles:
+        p.update()
+    assert np.abs(_stack(lbm, "lx") - np.concatenate([p.lx for p in ref.particles])).max() < 1e-5
+    for s in range(2):
+        run(lbm, 1)
+        ref.run_step()
+        ref.step += 1
+        for k in ("cx", "cu", "cw"):
+            got = _stack(lbm, k)
+            want = np.stack([getattr(p, k) for p in ref.particles])
+            assert np.abs(got - want).max() <= 1e-4 * max(1.0, np.abs(want).max()), (s, k)
+        lf = np.concatenate([p.lF for p in ref.particles])
+        assert np.abs(_stack(lbm, "lF") - lf).max() <= 1e-4 * np.abs(lf).max(), s
+        fol = ref.flow.FOL
+        assert np.abs(to_np(lbm.flow.FOL) - fol).max() <= 1e-4 * np.abs(fol).max(), s
+        assert rel_err(to_np(lbm.flow.rou), ref.flow.rou) < 2e-5
 
 
 def test_reference_mode_is_deterministic():
