@@ -41,6 +41,8 @@ class LbmLattice(ctypes.Structure):
         ("storage", ctypes.c_int32),
         ("re_mu", ctypes.c_float),
         ("neq_profile", ctypes.c_void_p),
+        ("step_nodes", ctypes.c_int32),
+        ("step_threads", ctypes.c_int32),
     ]
 
 

@@ -99,6 +99,147 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Vectorised fused step: thread = NZ consecutive nodes of one z-row (nz a
+// multiple of NZ), populations moved as NZ-element vectors (16 / 8 byte
+// loads and stores).  For rows whose (x, y) is interior every source of
+// direction i lies in row (x - ex, y - ey): one aligned vector load gives
+// NZ - |ez| of the NZ values, one scalar load the remaining one -- from the
+// neighbouring vector, or at z = 0 / z = nz - 1 from the bottom / top face
+// rule.  Rows on an x / y face take the per-node face rules.
+// ---------------------------------------------------------------------------
+template <int Q, int S, int NZ>
+__device__ __forceinline__ float zface_value(const typename Storage<S>::T *__restrict__ fa,
+                                             const Geom &g, int i, int rev, float w, long long row,
+                                             int fc, int x, int y, int z,
+                                             const float *__restrict__ face_rho, float eu) {
+  const int code = g.face[fc];
+  if (code == LBM_BC_PERIODICAL) {
+    // z moved to the opposite plane, same x and y
+    const int zs = (fc == 4) ? g.nz - 1 : 0;
+    return Storage<S>::load(fa + (long long)i * g.n + row + zs, w);
+  }
+  float v = Storage<S>::load(fa + (long long)rev * g.n + row + z, w);
+  if (code == LBM_BC_WALL_WITH_SPEED)
+    v -= 2.f * (face_rho[plane_index(g, fc, x, y, z)] * w) * eu * g.inv_cs2;
+  return v;
+}
+
+template <int Q, int S, bool FORCE, int NZ, int TB>
+__global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  constexpr int kWords = NZ * St::kBits / 32;
+  const unsigned t = blockIdx.x * TB + threadIdx.x;
+  const unsigned idx0 = t * NZ;
+  if (idx0 >= (unsigned)a.g.n) return;
+  int x, y, z0;
+  a.dec(idx0, x, y, z0);
+  const T *__restrict__ fa = static_cast<const T *>(a.fa);
+  const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
+  float f[NZ][Q];
+  if (row_in) {
+    const long long row = (long long)idx0 - z0;
+    const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int ex = V::ex(i), ey = V::ey(i), ez = V::ez(i);
+      constexpr float w = V::w(i);
+      const long long src = (long long)i * a.g.n + idx0 - ((long long)ex * a.g.nyz + (long long)ey * a.g.nz);
+      const Words<kWords> raw = ld_words<kWords>(fa + src);
+      float v[NZ];
+#pragma unroll
+      for (int k = 0; k < NZ; ++k)
+        v[k] = St::from_bits(St::kBits == 32 ? raw.w[k] : (raw.w[k >> 1] >> (16 * (k & 1))), w);
+      if (ez == 0) {
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) f[k][i] = v[k];
+      } else if (ez > 0) {
+#pragma unroll
+        for (int k = 1; k < NZ; ++k) f[k][i] = v[k - 1];
+        if (bottom) {
+          const float eu = (float)ex * a.g.uw[4][0] + (float)ey * a.g.uw[4][1] + (float)ez * a.g.uw[4][2];
+          f[0][i] = zface_value<Q, S, NZ>(fa, a.g, i, V::rev(i), w, row, 4, x, y, 0, a.face_rho_in, eu);
+        } else {
+          f[0][i] = St::load(fa + src - 1, w);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < NZ - 1; ++k) f[k][i] = v[k + 1];
+        if (top) {
+          const float eu = (float)ex * a.g.uw[5][0] + (float)ey * a.g.uw[5][1] + (float)ez * a.g.uw[5][2];
+          f[NZ - 1][i] = zface_value<Q, S, NZ>(fa, a.g, i, V::rev(i), w, row, 5, x, y, a.g.nz - 1,
+                                               a.face_rho_in, eu);
+        } else {
+          f[NZ - 1][i] = St::load(fa + src + NZ, w);
+        }
+      }
+    });
+  } else {
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) pull_general<Q, S>(fa, a.g, x, y, z0 + k, a.face_rho_in, f[k]);
+  }
+
+#pragma unroll
+  for (int k = 0; k < NZ; ++k) {
+    const unsigned idx = idx0 + k;
+    const int z = z0 + k;
+    const bool face = !row_in || z == 0 || z == a.g.nz - 1;
+    float fox = a.go[0], foy = a.go[1], foz = a.go[2];
+    float fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
+    if (a.fol_old != nullptr && (a.ch_old == nullptr || a.ch_old[idx >> 5])) {
+      fox += a.fol_old[3ull * idx];
+      foy += a.fol_old[3ull * idx + 1];
+      foz += a.fol_old[3ull * idx + 2];
+    }
+    if (a.fol_new != nullptr && (a.ch_new == nullptr || a.ch_new[idx >> 5])) {
+      fnx += a.fol_new[3ull * idx];
+      fny += a.fol_new[3ull * idx + 1];
+      fnz += a.fol_new[3ull * idx + 2];
+    }
+    float rho, ux, uy, uz;
+    moments<Q>(f[k], fox, foy, foz, face, rho, ux, uy, uz);
+    if (FORCE) {
+      add_force<Q>(f[k], a.g, ux, uy, uz, fnx, fny, fnz);
+      moments<Q>(f[k], fnx, fny, fnz, face, rho, ux, uy, uz);
+    }
+    flag_bad(a.status, rho, ux, uy, uz);
+    if (face && a.face_rho_out != nullptr) write_face_rho<Q>(a.g, a.face_rho_out, x, y, z, rho);
+    if (a.obs_f != nullptr) {
+      static_for<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        a.obs_f[(long long)i * a.g.n + idx] = f[k][i];
+      });
+    }
+    if (a.obs_rho != nullptr) a.obs_rho[idx] = rho;
+    if (a.obs_u != nullptr) {
+      a.obs_u[3ull * idx] = ux;
+      a.obs_u[3ull * idx + 1] = uy;
+      a.obs_u[3ull * idx + 2] = uz;
+    }
+    if (a.fb != nullptr) collide<Q>(f[k], a.g, rho, ux, uy, uz);
+  }
+  if (a.fb == nullptr) return;
+  T *__restrict__ fb = static_cast<T *>(a.fb);
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr float w = V::w(i);
+    Words<kWords> raw;
+#pragma unroll
+    for (int j = 0; j < kWords; ++j) raw.w[j] = 0u;
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      const unsigned b = St::to_bits(f[k][i], w);
+      if (St::kBits == 32)
+        raw.w[k] = b;
+      else
+        raw.w[k >> 1] |= b << (16 * (k & 1));
+    }
+    st_words(fb + (long long)i * a.g.n + idx0, raw);
+  });
+}
+
+// ---------------------------------------------------------------------------
 // Initialisation: f = f0 (or w), moments with FOL = 0 and the face rule,
 // then two collisions with those same moments (LBMD3._init's cul_equ and
 // step 1's cul_equ, which the reference runs before refreshing the moments).
@@ -280,21 +421,63 @@ int dispatch_q(int q, A &&...args) {
   }
 }
 
+// Launch shape of the fused step: nodes per thread (1 = scalar kernel, or
+// NZ consecutive z-nodes moved as vectors, nz a multiple of NZ) and threads
+// per block.  `nodes` == 0 picks the widest 16-byte vector the row allows.
+template <int S>
+constexpr int vec_width_max() {
+  return Storage<S>::kBits == 32 ? 4 : 8;
+}
+
+inline bool step_shape_ok(int nodes, int nz, int bits) {
+  if (nodes == 1) return true;
+  if (nodes != 2 && nodes != 4 && nodes != 8) return false;
+  if (nodes * bits / 32 < 1 || nodes * bits / 32 > 4) return false;
+  return nz % nodes == 0 && nz >= 2 * nodes;
+}
+
 template <int Q>
 struct RunStep {
+  template <int S, int NZ, int TB>
+  static void go_vec(const StepArgs &a, bool force, cudaStream_t s) {
+    const unsigned nb = blocks_for(a.g.n / NZ, TB);
+    if (force)
+      k_step_vec<Q, S, true, NZ, TB><<<nb, TB, 0, s>>>(a);
+    else
+      k_step_vec<Q, S, false, NZ, TB><<<nb, TB, 0, s>>>(a);
+  }
+  template <int S, int NZ>
+  static void go_nz(const StepArgs &a, bool force, int threads, cudaStream_t s) {
+    if (threads == 128)
+      go_vec<S, NZ, 128>(a, force, s);
+    else
+      go_vec<S, NZ, 256>(a, force, s);
+  }
   template <int S>
-  static void go(const StepArgs &a, bool force, cudaStream_t s) {
+  static void go(const StepArgs &a, bool force, int nodes, int threads, cudaStream_t s) {
+    constexpr int W = vec_width_max<S>();
+    if (nodes == 0) nodes = step_shape_ok(W, a.g.nz, Storage<S>::kBits) ? W
+                           : step_shape_ok(W / 2, a.g.nz, Storage<S>::kBits) ? W / 2 : 1;
+    if (nodes == W) {
+      go_nz<S, W>(a, force, threads, s);
+      return;
+    }
+    if (nodes == W / 2) {
+      go_nz<S, W / 2>(a, force, threads, s);
+      return;
+    }
     const unsigned nb = blocks_for(a.g.n, kThreads);
     if (force)
       k_step<Q, S, true><<<nb, kThreads, 0, s>>>(a);
     else
       k_step<Q, S, false><<<nb, kThreads, 0, s>>>(a);
   }
-  static int run(const StepArgs &a, int storage, bool force, cudaStream_t s) {
+  static int run(const StepArgs &a, int storage, bool force, int nodes, int threads,
+                 cudaStream_t s) {
     switch (storage) {
-      case LBM_STORAGE_FP32: go<LBM_STORAGE_FP32>(a, force, s); break;
-      case LBM_STORAGE_FP16S: go<LBM_STORAGE_FP16S>(a, force, s); break;
-      default: go<LBM_STORAGE_BF16S>(a, force, s); break;
+      case LBM_STORAGE_FP32: go<LBM_STORAGE_FP32>(a, force, nodes, threads, s); break;
+      case LBM_STORAGE_FP16S: go<LBM_STORAGE_FP16S>(a, force, nodes, threads, s); break;
+      default: go<LBM_STORAGE_BF16S>(a, force, nodes, threads, s); break;
     }
     LBM_LAUNCH_CHECK("lbm_flow_step");
     return LBM_OK;
@@ -433,7 +616,18 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
     a.obs_u = obs->u;
   }
   a.status = status;
-  return dispatch_q<RunStep>(lat->q, a, lat->storage, use_force, (cudaStream_t)stream);
+  const int bits = lat->storage == LBM_STORAGE_FP32 ? 32 : 16;
+  if (lat->step_nodes != 0 && !step_shape_ok(lat->step_nodes, lat->nz, bits)) {
+    set_error("lbm_flow_step: %d nodes per thread does not fit rows of %d nodes (%d-bit storage)",
+              lat->step_nodes, lat->nz, bits);
+    return LBM_ERR_INVALID;
+  }
+  if (lat->step_threads != 0 && lat->step_threads != 128 && lat->step_threads != 256) {
+    set_error("lbm_flow_step: step_threads must be 128 or 256");
+    return LBM_ERR_INVALID;
+  }
+  return dispatch_q<RunStep>(lat->q, a, lat->storage, use_force, (int)lat->step_nodes,
+                             (int)lat->step_threads, (cudaStream_t)stream);
 }
 
 int lbm_collide(const lbm_lattice *lat, float *f, const float *rho, const float *u, float *feq,

@@ -113,32 +113,82 @@ struct VSet<27> {
 template <int S>
 struct Storage;
 
+// from_bits / to_bits convert one stored element held in the low bits of a
+// 32-bit word (used by the vectorised loads and stores).
 template <>
 struct Storage<LBM_STORAGE_FP32> {
   using T = float;
+  static constexpr int kBits = 32;
   __device__ __forceinline__ static float load(const T *p, float) { return __ldg(p); }
   __device__ __forceinline__ static void store(T *p, float v, float) { *p = v; }
+  __device__ __forceinline__ static float from_bits(unsigned b, float) { return __uint_as_float(b); }
+  __device__ __forceinline__ static unsigned to_bits(float v, float) { return __float_as_uint(v); }
 };
 template <>
 struct Storage<LBM_STORAGE_FP16S> {
   using T = __half;
+  static constexpr int kBits = 16;
   __device__ __forceinline__ static float load(const T *p, float w) {
     return w + __half2float(__ldg(p));
   }
   __device__ __forceinline__ static void store(T *p, float v, float w) {
     *p = __float2half_rn(v - w);
   }
+  __device__ __forceinline__ static float from_bits(unsigned b, float w) {
+    return w + __half2float(__ushort_as_half((unsigned short)(b & 0xffffu)));
+  }
+  __device__ __forceinline__ static unsigned to_bits(float v, float w) {
+    return (unsigned)__half_as_ushort(__float2half_rn(v - w));
+  }
 };
 template <>
 struct Storage<LBM_STORAGE_BF16S> {
   using T = __nv_bfloat16;
+  static constexpr int kBits = 16;
   __device__ __forceinline__ static float load(const T *p, float w) {
     return w + __bfloat162float(__ldg(p));
   }
   __device__ __forceinline__ static void store(T *p, float v, float w) {
     *p = __float2bfloat16_rn(v - w);
   }
+  __device__ __forceinline__ static float from_bits(unsigned b, float w) {
+    return w + __bfloat162float(__ushort_as_bfloat16((unsigned short)(b & 0xffffu)));
+  }
+  __device__ __forceinline__ static unsigned to_bits(float v, float w) {
+    return (unsigned)__bfloat16_as_ushort(__float2bfloat16_rn(v - w));
+  }
 };
+
+// Aligned vector loads / stores of WORDS 32-bit words (4, 8 or 16 bytes).
+template <int WORDS>
+struct Words {
+  unsigned w[WORDS];
+};
+template <int WORDS>
+__device__ __forceinline__ Words<WORDS> ld_words(const void *p);
+template <>
+__device__ __forceinline__ Words<1> ld_words<1>(const void *p) {
+  return Words<1>{{__ldg(static_cast<const unsigned *>(p))}};
+}
+template <>
+__device__ __forceinline__ Words<2> ld_words<2>(const void *p) {
+  const uint2 v = __ldg(static_cast<const uint2 *>(p));
+  return Words<2>{{v.x, v.y}};
+}
+template <>
+__device__ __forceinline__ Words<4> ld_words<4>(const void *p) {
+  const uint4 v = __ldg(static_cast<const uint4 *>(p));
+  return Words<4>{{v.x, v.y, v.z, v.w}};
+}
+__device__ __forceinline__ void st_words(void *p, const Words<1> &v) {
+  *static_cast<unsigned *>(p) = v.w[0];
+}
+__device__ __forceinline__ void st_words(void *p, const Words<2> &v) {
+  *static_cast<uint2 *>(p) = make_uint2(v.w[0], v.w[1]);
+}
+__device__ __forceinline__ void st_words(void *p, const Words<4> &v) {
+  *static_cast<uint4 *>(p) = make_uint4(v.w[0], v.w[1], v.w[2], v.w[3]);
+}
 
 // ---------------------------------------------------------------------------
 // Lattice constants passed by value to every kernel.

@@ -157,6 +157,17 @@ class Lattice:
              None if force is None else ctypes_ref(force), ptr(self.face_rho[prev]), None,
              ctypes_ref(obs), None, self.stream())
 
+    def set_launch_shape(self, nodes=0, threads=0):
+        """Launch shape of the fused step (see funlbm_b200.tune)."""
+        for d in (self.desc,):
+            d.step_nodes = int(nodes)
+            d.step_threads = int(threads)
+
+    def tune(self, force=None, verbose=False):
+        from .tune import tune
+
+        return tune(self, force=force, verbose=verbose)
+
     def read_status(self, reset=True):
         v = int(self.status.item())
         if reset:

@@ -1,0 +1,76 @@
+"""Launch-shape autotuner of the fused step kernel.
+
+The fused step can run one node per thread or NZ consecutive z-nodes per
+thread moved as 8 / 16-byte vectors, with 128 or 256 threads per block.  The
+best shape depends on the velocity set, the storage type and the row length,
+so ``tune`` times every legal candidate with CUDA events on a scratch lattice
+of the same velocity set, storage, faces and (ny, nz) -- with nx cut down so
+the proxy still holds several times the L2 -- and caches the winner per
+(q, storage, ny, nz, forced).  Tuning never touches the caller's populations.
+"""
+from __future__ import annotations
+
+import torch
+
+CANDIDATES = {
+    32: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256)],
+    16: [(1, 256), (4, 128), (4, 256), (8, 128), (8, 256)],
+}
+_CACHE = {}
+PROXY_BYTES = 2 << 30          # populations of the proxy lattice (both buffers)
+
+
+def shape_ok(nodes, nz, bits):
+    if nodes == 1:
+        return True
+    if nodes * bits // 32 not in (1, 2, 4):
+        return False
+    return nz % nodes == 0 and nz >= 2 * nodes
+
+
+def tune(lat, force=None, iters=6, warmup=2, verbose=False):
+    """Choose (nodes per thread, threads per block) for ``lat`` and store it
+    in its descriptor.  Returns the choice and the timings in ms per step."""
+    from .lattice import BYTES, Lattice
+
+    bits = 32 if lat.storage == "fp32" else 16
+    key = (lat.q, lat.storage, lat.shape[1], lat.shape[2], force is not None)
+    if key in _CACHE:
+        choice, timings = _CACHE[key]
+        lat.set_launch_shape(*choice)
+        return choice, timings
+    nx, ny, nz = lat.shape
+    per_x = 2 * lat.q * ny * nz * BYTES[lat.storage]
+    px = max(4, min(nx, PROXY_BYTES // max(per_x, 1)))
+    proxy = Lattice(lat.q, (px, ny, nz), lat.faces, lat.tau, storage=lat.storage,
+                    face_uw=lat.face_uw, re_mu=lat.re_mu, device=lat.device)
+    proxy.init(None)
+    timings = {}
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    for nodes, threads in CANDIDATES[bits]:
+        if not shape_ok(nodes, nz, bits):
+            continue
+        proxy.set_launch_shape(nodes, threads)
+        for _ in range(warmup):
+            proxy.step(force)
+        start.record()
+        for _ in range(iters):
+            proxy.step(force)
+        stop.record()
+        stop.synchronize()
+        timings[(nodes, threads)] = start.elapsed_time(stop) / iters
+    proxy.release()
+    del proxy
+    choice = min(timings, key=timings.get)
+    if verbose:
+        for k, v in sorted(timings.items(), key=lambda kv: kv[1]):
+            print("tune q=%d %s %dx%dx%d (proxy nx=%d): nodes=%d threads=%d  %.4f ms"
+                  % (lat.q, lat.storage, nx, ny, nz, px, k[0], k[1], v))
+    _CACHE[key] = (choice, timings)
+    lat.set_launch_shape(*choice)
+    return choice, timings
+
+
+def clear_cache():
+    _CACHE.clear()

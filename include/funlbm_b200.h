@@ -70,6 +70,9 @@ typedef struct lbm_lattice {
   float re_mu;            /* Re * mu, NON_EQUILIBRIUM inlet scale (flow/d3/base.py:137-143) */
   const double *neq_profile; /* device [ny*nz] duct profile init_u / u_max (float64, */
                              /* as cul_u returns it); NULL unless face[0] is NEQ    */
+  int32_t step_nodes;     /* launch shape of lbm_flow_step: consecutive z-nodes per  */
+                          /* thread (1, 2, 4, 8; 0 = choose from the row length)    */
+  int32_t step_threads;   /* threads per block (128 or 256; 0 = 256)                */
 } lbm_lattice;
 
 /* Forcing seen by one step: FOL = uniform + field.  `uniform` is a body force

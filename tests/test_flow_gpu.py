@@ -300,3 +300,40 @@ def test_shifted_storage_vs_fp64(storage, bound):
     e_u = np.abs(u - ref.u).max() / np.abs(ref.u).max()
     print("%s: rho err %.2e, u err %.2e" % (storage, e_rho, e_u))
     assert e_rho <= bound and e_u <= bound
+
+
+@pytest.mark.parametrize("q", [13, 15, 19, 27])
+@pytest.mark.parametrize("storage", ["fp32", "fp16s", "bf16s"])
+def test_launch_shapes_agree_bitwise(q, storage):
+    """Every launch shape of the fused step (one node per thread, or 2 / 4 / 8
+    z-nodes per thread moved as vectors; 128 / 256 threads) gives bit-identical
+    results, face rules included (z faces are served by the vector path's
+    face-rule loads)."""
+    from funlbm_b200.lattice import Lattice, make_force, tau_float32
+    from funlbm_b200.tune import CANDIDATES, shape_ok
+
+    rng = np.random.default_rng(100 + q)
+    shape = (9, 7, 16)
+    codes = [int(c) for c in rng.choice([11000, 1200, 1201], 6)]
+    codes[4], codes[5] = 1201, 11000 if q % 2 else 1201
+    uw = (0.02 * rng.standard_normal((6, 3))).tolist()
+    f0 = smooth_f0(q, shape, 0.04, q)
+    f0_soa = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda")
+    bits = 32 if storage == "fp32" else 16
+    force = make_force((0, 0, 0), (1e-5, -2e-5, 3e-5))
+    results = {}
+    for nodes, threads in CANDIDATES[bits]:
+        if not shape_ok(nodes, shape[2], bits):
+            continue
+        lat = Lattice(q, shape, codes, tau_float32(0.07), storage=storage, face_uw=uw, device="cuda")
+        lat.set_launch_shape(nodes, threads)
+        lat.init(f0_soa)
+        for _ in range(4):
+            lat.step(force)
+        f = torch.empty(q * lat.n, device="cuda")
+        lat.observe(force, f=f)
+        results[(nodes, threads)] = to_np(f)
+    assert len(results) >= 3
+    ref = results[(1, 256)]
+    for k, v in results.items():
+        assert np.array_equal(v, ref), (k, np.abs(v - ref).max())
