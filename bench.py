@@ -185,6 +185,7 @@ def run_device(args, world, rank, local):
     f0 = taylor_green_soa(lat, torch)
     lat.init(f0)
     del f0
+    shape, _ = lat.tune()          # launch-shape autotuner (scratch proxy lattice)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         lat.step(None)
@@ -209,7 +210,7 @@ def run_device(args, world, rank, local):
     lat.release()
     del lat
     torch.cuda.empty_cache()
-    return ms_max, clocks, status
+    return ms_max, clocks, status, shape
 
 
 def run_e2e(args, world, local):
@@ -380,7 +381,7 @@ def main():
     build.build()
     world, rank, local = dist_setup(args)
     n = args.size
-    ms, clocks, status = run_device(args, world, rank, local)
+    ms, clocks, status, launch = run_device(args, world, rank, local)
     ms_per_step = ms / args.steps
     nodes = n ** 3
     value = world * nodes * args.steps / (ms / 1e3) / 1e6
@@ -412,6 +413,8 @@ def main():
         "config": {"workload": "D3Q19 %s, %d^3 nodes, all faces periodic, tau 0.6, Taylor-Green "
                                "u0=0.05; replicas per GPU" % (args.storage, n),
                    "nodes_per_gpu": nodes, "parallelism": "replicas",
+                   "launch_shape": {"nodes_per_thread": launch[0], "threads_per_block": launch[1],
+                                    "chosen_by": "funlbm_b200.tune"},
                    "l2_flush": "not needed: %.1f GB of populations per step >> 126 MB L2"
                                % (2 * bytes_per_launch / 2 / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

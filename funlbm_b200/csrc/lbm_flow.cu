@@ -148,9 +148,17 @@ __global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
       const long long src = (long long)i * a.g.n + idx0 - ((long long)ex * a.g.nyz + (long long)ey * a.g.nz);
       const Words<kWords> raw = ld_words<kWords>(fa + src);
       float v[NZ];
+      if constexpr (St::kBits == 32) {
 #pragma unroll
-      for (int k = 0; k < NZ; ++k)
-        v[k] = St::from_bits(St::kBits == 32 ? raw.w[k] : (raw.w[k >> 1] >> (16 * (k & 1))), w);
+        for (int k = 0; k < NZ; ++k) v[k] = __uint_as_float(raw.w[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < NZ / 2; ++k) {
+          const float2 p2 = unpack2<S>(raw.w[k], w);
+          v[2 * k] = p2.x;
+          v[2 * k + 1] = p2.y;
+        }
+      }
       if (ez == 0) {
 #pragma unroll
         for (int k = 0; k < NZ; ++k) f[k][i] = v[k];
@@ -225,15 +233,12 @@ __global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
     constexpr int i = decltype(ic)::value;
     constexpr float w = V::w(i);
     Words<kWords> raw;
+    if constexpr (St::kBits == 32) {
 #pragma unroll
-    for (int j = 0; j < kWords; ++j) raw.w[j] = 0u;
+      for (int k = 0; k < NZ; ++k) raw.w[k] = __float_as_uint(f[k][i]);
+    } else {
 #pragma unroll
-    for (int k = 0; k < NZ; ++k) {
-      const unsigned b = St::to_bits(f[k][i], w);
-      if (St::kBits == 32)
-        raw.w[k] = b;
-      else
-        raw.w[k >> 1] |= b << (16 * (k & 1));
+      for (int k = 0; k < NZ / 2; ++k) raw.w[k] = pack2<S>(f[2 * k][i], f[2 * k + 1][i], w);
     }
     st_words(fb + (long long)i * a.g.n + idx0, raw);
   });
@@ -276,14 +281,23 @@ __global__ void __launch_bounds__(kThreads)
   const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= (unsigned)g.n) return;
   const float r = rho[idx], ux = u[3ull * idx], uy = u[3ull * idx + 1], uz = u[3ull * idx + 2];
-  const float u2 = (ux * ux + uy * uy + uz * uz) * 0.5f * g.inv_cs2;
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const long long k = (long long)i * g.n + idx;
-    const float fe = feq_of<Q>(g, i, r, ux, uy, uz, u2);
-    if (feq != nullptr) feq[k] = fe;
-    f[k] = f[k] - (f[k] - fe) * g.inv_tau;
+  float fl[Q];
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    fl[i] = f[(long long)i * g.n + idx];
+  });
+  if (feq != nullptr) {
+    const float u2 = LBM_FMA(ux, ux, LBM_FMA(uy, uy, uz * uz)) * (0.5f * g.inv_cs2);
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      feq[(long long)i * g.n + idx] = feq_of<Q>(g, i, r, ux, uy, uz, u2);
+    });
   }
+  collide<Q>(fl, g, r, ux, uy, uz);
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    f[(long long)i * g.n + idx] = fl[i];
+  });
 }
 
 // f_stream + f_stream_bound_* with every face code, NON_EQUILIBRIUM included.
@@ -422,13 +436,8 @@ int dispatch_q(int q, A &&...args) {
 }
 
 // Launch shape of the fused step: nodes per thread (1 = scalar kernel, or
-// NZ consecutive z-nodes moved as vectors, nz a multiple of NZ) and threads
-// per block.  `nodes` == 0 picks the widest 16-byte vector the row allows.
-template <int S>
-constexpr int vec_width_max() {
-  return Storage<S>::kBits == 32 ? 4 : 8;
-}
-
+// NZ consecutive z-nodes moved as 4 / 8 / 16-byte vectors, nz a multiple of
+// NZ) and threads per block.
 inline bool step_shape_ok(int nodes, int nz, int bits) {
   if (nodes == 1) return true;
   if (nodes != 2 && nodes != 4 && nodes != 8) return false;
@@ -455,16 +464,26 @@ struct RunStep {
   }
   template <int S>
   static void go(const StepArgs &a, bool force, int nodes, int threads, cudaStream_t s) {
-    constexpr int W = vec_width_max<S>();
-    if (nodes == 0) nodes = step_shape_ok(W, a.g.nz, Storage<S>::kBits) ? W
-                           : step_shape_ok(W / 2, a.g.nz, Storage<S>::kBits) ? W / 2 : 1;
-    if (nodes == W) {
-      go_nz<S, W>(a, force, threads, s);
+    constexpr int bits = Storage<S>::kBits;
+    if (nodes == 0) {
+      // measured on B200: 2 nodes per thread with 128-thread blocks is the
+      // fastest shape for every velocity set in float32 (see funlbm_b200.tune)
+      nodes = step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
+      threads = threads ? threads : 128;
+    }
+    if (nodes == 2) {
+      go_nz<S, 2>(a, force, threads, s);
       return;
     }
-    if (nodes == W / 2) {
-      go_nz<S, W / 2>(a, force, threads, s);
+    if (nodes == 4) {
+      go_nz<S, 4>(a, force, threads, s);
       return;
+    }
+    if constexpr (bits == 16) {
+      if (nodes == 8) {
+        go_nz<S, 8>(a, force, threads, s);
+        return;
+      }
     }
     const unsigned nb = blocks_for(a.g.n, kThreads);
     if (force)

@@ -159,6 +159,37 @@ struct Storage<LBM_STORAGE_BF16S> {
   }
 };
 
+// Two consecutive 16-bit elements in one 32-bit word (low half first).
+template <int S>
+__device__ __forceinline__ float2 unpack2(unsigned word, float w);
+template <>
+__device__ __forceinline__ float2 unpack2<LBM_STORAGE_FP16S>(unsigned word, float w) {
+  __half2 h;
+  memcpy(&h, &word, 4);
+  const float2 v = __half22float2(h);
+  return make_float2(v.x + w, v.y + w);
+}
+template <>
+__device__ __forceinline__ float2 unpack2<LBM_STORAGE_BF16S>(unsigned word, float w) {
+  return make_float2(__uint_as_float(word << 16) + w, __uint_as_float(word & 0xffff0000u) + w);
+}
+template <int S>
+__device__ __forceinline__ unsigned pack2(float a, float b, float w);
+template <>
+__device__ __forceinline__ unsigned pack2<LBM_STORAGE_FP16S>(float a, float b, float w) {
+  const __half2 h = __floats2half2_rn(a - w, b - w);
+  unsigned word;
+  memcpy(&word, &h, 4);
+  return word;
+}
+template <>
+__device__ __forceinline__ unsigned pack2<LBM_STORAGE_BF16S>(float a, float b, float w) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a - w, b - w);
+  unsigned word;
+  memcpy(&word, &h, 4);
+  return word;
+}
+
 // Aligned vector loads / stores of WORDS 32-bit words (4, 8 or 16 bytes).
 template <int WORDS>
 struct Words {
@@ -326,67 +357,130 @@ __device__ __forceinline__ float pull_rolled(const typename Storage<S>::T *__res
 }
 
 // ---------------------------------------------------------------------------
+// Per-node arithmetic.  Directions come in opposite pairs (i, rev(i)); the
+// moments, the forcing term and the equilibrium share their work across the
+// pair.  The library is built with -fmad=false and every fused multiply-add
+// below is explicit (__fmaf_rn), so each kernel that calls these functions
+// produces the same bits whatever its launch shape.
+// ---------------------------------------------------------------------------
+#define LBM_FMA(a, b, c) __fmaf_rn((a), (b), (c))
+
 // Moments (flow/d3/base.py:116-133): rho = sum f, u = (sum f e + F/2) / rho,
 // u := 0 on all six boundary planes whatever their condition.
-// ---------------------------------------------------------------------------
 template <int Q>
 __device__ __forceinline__ void moments(const float f[Q], float fx, float fy, float fz,
                                         bool face, float &rho, float &ux, float &uy, float &uz) {
   using V = VSet<Q>;
-  float r = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+  float r = f[0], jx = 0.f, jy = 0.f, jz = 0.f;
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    r += f[i];
-    if (V::ex(i) > 0) jx += f[i];
-    if (V::ex(i) < 0) jx -= f[i];
-    if (V::ey(i) > 0) jy += f[i];
-    if (V::ey(i) < 0) jy -= f[i];
-    if (V::ez(i) > 0) jz += f[i];
-    if (V::ez(i) < 0) jz -= f[i];
+    constexpr int j = V::rev(i);
+    if constexpr (i != 0 && i < j) {
+      const float s = f[i] + f[j];
+      const float d = f[i] - f[j];
+      r += s;
+      if constexpr (V::ex(i) > 0) jx += d;
+      if constexpr (V::ex(i) < 0) jx -= d;
+      if constexpr (V::ey(i) > 0) jy += d;
+      if constexpr (V::ey(i) < 0) jy -= d;
+      if constexpr (V::ez(i) > 0) jz += d;
+      if constexpr (V::ez(i) < 0) jz -= d;
+    }
   });
   rho = r;
   const float inv = 1.f / r;
-  ux = face ? 0.f : (jx + 0.5f * fx) * inv;
-  uy = face ? 0.f : (jy + 0.5f * fy) * inv;
-  uz = face ? 0.f : (jz + 0.5f * fz) * inv;
+  ux = face ? 0.f : LBM_FMA(0.5f, fx, jx) * inv;
+  uy = face ? 0.f : LBM_FMA(0.5f, fy, jy) * inv;
+  uz = face ? 0.f : LBM_FMA(0.5f, fz, jz) * inv;
+}
+
+// e_i . v with e_i in {-1, 0, 1}^3, folded at compile time
+template <int Q, int I>
+__device__ __forceinline__ float edot(float vx, float vy, float vz) {
+  using V = VSet<Q>;
+  float r = 0.f;
+  bool first = true;
+  auto acc = [&](int e, float v) {
+    if (e == 0) return;
+    if (first) {
+      r = e > 0 ? v : -v;
+      first = false;
+    } else {
+      r = e > 0 ? r + v : r - v;
+    }
+  };
+  acc(V::ex(I), vx);
+  acc(V::ey(I), vy);
+  acc(V::ez(I), vz);
+  return r;
 }
 
 // Forcing term of FlowD3.cul_equ2 (flow/d3/base.py:103-114):
 //   f_i += (1 - 1/(2 tau)) w_i [ (e_i - u)/cs^2 + (u o e_i) o e_i / cs^4 ] . F
-// (component-wise u_k e_ik^2, the reference's form).
+// (component-wise u_k e_ik^2, the reference's form).  For the pair (i, j),
+// e_j = -e_i: the e.F part flips sign, the rest is shared.
 template <int Q>
 __device__ __forceinline__ void add_force(float f[Q], const Geom &g, float ux, float uy, float uz,
                                           float fx, float fy, float fz) {
   using V = VSet<Q>;
-  const float uF = ux * fx + uy * fy + uz * fz;
+  const float uF = LBM_FMA(ux, fx, LBM_FMA(uy, fy, uz * fz));
   const float ax = ux * fx, ay = uy * fy, az = uz * fz;
+  const float base = -uF * g.inv_cs2;
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const float eF = (float)V::ex(i) * fx + (float)V::ey(i) * fy + (float)V::ez(i) * fz;
-    const float t2 = (V::ex(i) ? ax : 0.f) + (V::ey(i) ? ay : 0.f) + (V::ez(i) ? az : 0.f);
-    f[i] += g.force_c * V::w(i) * ((eF - uF) * g.inv_cs2 + t2 * g.inv_cs4);
+    constexpr int j = V::rev(i);
+    constexpr float cw = V::w(i);
+    if constexpr (i == 0) {
+      f[0] = LBM_FMA(g.force_c * cw, base, f[0]);
+    } else if constexpr (i < j) {
+      float t2 = 0.f;
+      if constexpr (V::ex(i) != 0) t2 += ax;
+      if constexpr (V::ey(i) != 0) t2 += ay;
+      if constexpr (V::ez(i) != 0) t2 += az;
+      const float shared = LBM_FMA(t2, g.inv_cs4, base);
+      const float eF = edot<Q, i>(fx, fy, fz) * g.inv_cs2;
+      const float c = g.force_c * cw;
+      f[i] = LBM_FMA(c, shared + eF, f[i]);
+      f[j] = LBM_FMA(c, shared - eF, f[j]);
+    }
   });
 }
 
 // BGK collision of FlowD3.cul_equ (flow/d3/base.py:150-159):
 //   feq_i = (1 + t + t^2/2 - |u|^2/(2 cs^2)) rho w_i,  t = e_i.u / cs^2
-//   f_i  <- f_i - (f_i - feq_i) / tau
+//   f_i  <- f_i - (f_i - feq_i) / tau = f_i (1 - 1/tau) + feq_i / tau
+// With a = rho w (1 - |u|^2/(2cs^2) + t^2/2) and b = rho w t, the pair gets
+// feq_i = a + b, feq_rev(i) = a - b.
 template <int Q>
 __device__ __forceinline__ float feq_of(const Geom &g, int i, float rho, float ux, float uy,
                                         float uz, float u2) {
   using V = VSet<Q>;
   const float t = ((float)V::ex(i) * ux + (float)V::ey(i) * uy + (float)V::ez(i) * uz) * g.inv_cs2;
-  return (1.f + t + 0.5f * t * t - u2) * (rho * V::w(i));
+  return LBM_FMA(0.5f * t, t, (1.f - u2) + t) * (rho * V::w(i));
 }
 
 template <int Q>
 __device__ __forceinline__ void collide(float f[Q], const Geom &g, float rho, float ux, float uy,
                                         float uz) {
-  const float u2 = (ux * ux + uy * uy + uz * uz) * 0.5f * g.inv_cs2;
+  using V = VSet<Q>;
+  const float u2 = LBM_FMA(ux, ux, LBM_FMA(uy, uy, uz * uz)) * (0.5f * g.inv_cs2);
+  const float om = g.inv_tau, keep = 1.f - g.inv_tau;
+  const float orho = om * rho;
+  const float one_u2 = 1.f - u2;
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const float feq = feq_of<Q>(g, i, rho, ux, uy, uz, u2);
-    f[i] = f[i] - (f[i] - feq) * g.inv_tau;
+    constexpr int j = V::rev(i);
+    constexpr float w = V::w(i);
+    if constexpr (i == 0) {
+      f[0] = LBM_FMA(f[0], keep, (orho * w) * one_u2);
+    } else if constexpr (i < j) {
+      const float t = edot<Q, i>(ux, uy, uz) * g.inv_cs2;
+      const float ow = orho * w;
+      const float a = ow * LBM_FMA(0.5f * t, t, one_u2);
+      const float b = ow * t;
+      f[i] = LBM_FMA(f[i], keep, a + b);
+      f[j] = LBM_FMA(f[j], keep, a - b);
+    }
   });
 }
 

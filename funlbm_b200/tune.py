@@ -14,7 +14,7 @@ import torch
 
 CANDIDATES = {
     32: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256)],
-    16: [(1, 256), (4, 128), (4, 256), (8, 128), (8, 256)],
+    16: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256), (8, 128), (8, 256)],
 }
 _CACHE = {}
 PROXY_BYTES = 2 << 30          # populations of the proxy lattice (both buffers)
