@@ -20,6 +20,7 @@ LBM_ERR_CUDA = 3
 LBM_STATUS_RHO_BAD = 0x1
 LBM_STATUS_U_BAD = 0x2
 LBM_STATUS_STENCIL_EMPTY = 0x4
+LBM_STATUS_WAIT_TIMEOUT = 0x8
 
 STORAGE = {"fp32": 0, "fp16s": 1, "bf16s": 2}
 RIGID_WALL = 1

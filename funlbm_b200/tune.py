@@ -1,7 +1,9 @@
 """Launch-shape autotuner of the fused step kernel.
 
-The fused step can run one node per thread or NZ consecutive z-nodes per
-thread moved as 8 / 16-byte vectors, with 128 or 256 threads per block.  The
+The fused step can run one node per thread, NZ consecutive z-nodes per
+thread moved as 4 / 8 / 16-byte vectors (128 or 256 threads per block), or
+as a persistent kernel that stages whole z-rows in shared memory with TMA
+bulk copies.  The
 best shape depends on the velocity set, the storage type and the row length,
 so ``tune`` times every legal candidate with CUDA events on a scratch lattice
 of the same velocity set, storage, faces and (ny, nz) -- with nx cut down so
@@ -12,9 +14,10 @@ from __future__ import annotations
 
 import torch
 
+ROWS = -1   # whole z-rows staged in shared memory by TMA bulk copies
 CANDIDATES = {
-    32: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256)],
-    16: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256), (8, 128), (8, 256)],
+    32: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256), (ROWS, 256)],
+    16: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256), (8, 128), (8, 256), (ROWS, 256)],
 }
 _CACHE = {}
 PROXY_BYTES = 2 << 30          # populations of the proxy lattice (both buffers)
@@ -23,6 +26,8 @@ PROXY_BYTES = 2 << 30          # populations of the proxy lattice (both buffers)
 def shape_ok(nodes, nz, bits):
     if nodes == 1:
         return True
+    if nodes == ROWS:
+        return (nz * bits // 8) % 16 == 0 and nz >= 16
     if nodes * bits // 32 not in (1, 2, 4):
         return False
     return nz % nodes == 0 and nz >= 2 * nodes

@@ -40,6 +40,7 @@ extern "C" {
 #define LBM_STATUS_U_BAD 0x2u        /* velocity not finite at some node         */
 #define LBM_STATUS_STENCIL_EMPTY 0x4u /* a marker's normalised weight sum != 1   */
                                       /* after step 100 (lbm/lbm3d.py:84-86)     */
+#define LBM_STATUS_WAIT_TIMEOUT 0x8u  /* a bounded device-side wait gave up      */
 
 /* ---- boundary codes: values of funlbm's BoundaryCondition (config/base.py:17-23) */
 #define LBM_BC_PERIODICAL 11000
@@ -57,6 +58,8 @@ extern "C" {
 #define LBM_STORAGE_FP16S 1 /* float16 of (f_i - w_i), collided in float32       */
 #define LBM_STORAGE_BF16S 2 /* bfloat16 of (f_i - w_i), collided in float32      */
 
+#define LBM_STEP_ROWS (-1)
+
 /* One lattice: velocity set, shape, faces and relaxation.  Mirrors the
  * reference's FlowConfig + Param (flow/base.py:15-114, flow/d3/base.py:72-101). */
 typedef struct lbm_lattice {
@@ -71,7 +74,8 @@ typedef struct lbm_lattice {
   const double *neq_profile; /* device [ny*nz] duct profile init_u / u_max (float64, */
                              /* as cul_u returns it); NULL unless face[0] is NEQ    */
   int32_t step_nodes;     /* launch shape of lbm_flow_step: consecutive z-nodes per  */
-                          /* thread (1, 2, 4, 8; 0 = choose from the row length)    */
+                          /* thread (1, 2, 4, 8), LBM_STEP_ROWS (whole z-rows staged */
+                          /* in shared memory by TMA bulk copies), 0 = default      */
   int32_t step_threads;   /* threads per block (128 or 256; 0 = 256)                */
 } lbm_lattice;
 
