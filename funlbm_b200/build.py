@@ -4,7 +4,8 @@
     python -m funlbm_b200.build --force
 
 Each ``csrc/*.cu`` translation unit is compiled to an object in
-``funlbm_b200/_build/`` (in parallel) and linked into
+``funlbm_b200/_build/`` (in parallel; ``lbm_step_inst.cu`` once per velocity
+set and storage type) and linked into
 ``funlbm_b200/liblbm_b200.so`` with the CUDA runtime linked statically, so the
 library only needs the driver at run time.
 """
@@ -40,8 +41,26 @@ def _nvcc():
     return exe
 
 
+INSTANCED = "lbm_step_inst.cu"   # compiled once per (velocity set, storage)
+INSTANCES = [(q, st) for q in (13, 15, 19, 27) for st in (0, 1, 2)]
+
+
 def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def _units():
+    """(source, object, extra flags) of every translation unit."""
+    units = []
+    for src in _sources():
+        base = os.path.basename(src)[:-3]
+        if os.path.basename(src) == INSTANCED:
+            for q, st in INSTANCES:
+                units.append((src, os.path.join(BUILD, "%s_q%d_s%d.o" % (base, q, st)),
+                              ["-DLBM_Q=%d" % q, "-DLBM_S=%d" % st]))
+        else:
+            units.append((src, os.path.join(BUILD, base + ".o"), []))
+    return units
 
 
 def _deps():
@@ -62,11 +81,12 @@ def build(force=False, verbose=False, extra_flags=()):
         return LIB
     nvcc = _nvcc()
     os.makedirs(BUILD, exist_ok=True)
-    srcs = _sources()
-    objs = [os.path.join(BUILD, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    units = _units()
+    objs = [u[1] for u in units]
 
-    def compile_one(src, obj):
-        cmd = [nvcc, *ARCH, *FLAGS, *extra_flags, "-c", src, "-o", obj]
+    def compile_one(unit):
+        src, obj, defs = unit
+        cmd = [nvcc, *ARCH, *FLAGS, *extra_flags, *defs, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -74,8 +94,10 @@ def build(force=False, verbose=False, extra_flags=()):
             raise RuntimeError("nvcc failed on %s:\n%s%s" % (src, r.stdout, r.stderr))
         return obj
 
-    with cf.ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
-        list(ex.map(lambda so: compile_one(*so), zip(srcs, objs)))
+    # largest units first so the parallel build ends evenly
+    order = sorted(units, key=lambda u: 0 if u[2] else 1)
+    with cf.ThreadPoolExecutor(max_workers=min(len(units), os.cpu_count() or 4)) as ex:
+        list(ex.map(compile_one, order))
     tmp = LIB + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     if verbose:

@@ -1,0 +1,565 @@
+// Fused-step kernels (scalar, vectorised, TMA row-staged) and their launch
+// logic.  Included by lbm_flow.cu (declarations only) and by
+// lbm_step_inst.cu, which the build compiles once per (velocity set,
+// storage) with -DLBM_Q / -DLBM_S.
+#pragma once
+#include <algorithm>
+
+#include "lbm_api.cuh"
+#include "lbm_tma.cuh"
+
+namespace lbm {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Fused step
+// ---------------------------------------------------------------------------
+struct StepArgs {
+  Geom g;
+  NodeDecomp dec;
+  const void *fa;
+  void *fb;
+  float go[3], gn[3];
+  const float *fol_old, *fol_new;
+  const uint8_t *ch_old, *ch_new;
+  const float *face_rho_in;
+  float *face_rho_out;
+  float *obs_f, *obs_rho, *obs_u;
+  unsigned *status;
+};
+
+template <int Q>
+__device__ __forceinline__ void write_face_rho(const Geom &g, float *out, int x, int y, int z,
+                                               float rho) {
+  if (x == 0) out[plane_index(g, 0, x, y, z)] = rho;
+  if (x == g.nx - 1) out[plane_index(g, 1, x, y, z)] = rho;
+  if (y == 0) out[plane_index(g, 2, x, y, z)] = rho;
+  if (y == g.ny - 1) out[plane_index(g, 3, x, y, z)] = rho;
+  if (z == 0) out[plane_index(g, 4, x, y, z)] = rho;
+  if (z == g.nz - 1) out[plane_index(g, 5, x, y, z)] = rho;
+}
+
+// Everything after the pull for one node: the previous / new forcing, the
+// moment passes, cul_equ2, status, face densities, observation, and (when
+// fb is set) the next step's collision, in place in f.
+template <int Q, bool FORCE>
+__device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsigned idx, int x,
+                                            int y, int z, bool face) {
+  float fox = a.go[0], foy = a.go[1], foz = a.go[2];
+  float fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
+  if (a.fol_old != nullptr && (a.ch_old == nullptr || a.ch_old[idx >> 5])) {
+    fox += a.fol_old[3ull * idx];
+    foy += a.fol_old[3ull * idx + 1];
+    foz += a.fol_old[3ull * idx + 2];
+  }
+  if (a.fol_new != nullptr && (a.ch_new == nullptr || a.ch_new[idx >> 5])) {
+    fnx += a.fol_new[3ull * idx];
+    fny += a.fol_new[3ull * idx + 1];
+    fnz += a.fol_new[3ull * idx + 2];
+  }
+  float rho, ux, uy, uz;
+  moments<Q>(f, fox, foy, foz, face, rho, ux, uy, uz);
+  if (FORCE) {
+    add_force<Q>(f, a.g, ux, uy, uz, fnx, fny, fnz);
+    moments<Q>(f, fnx, fny, fnz, face, rho, ux, uy, uz);
+  }
+  flag_bad(a.status, rho, ux, uy, uz);
+  if (face && a.face_rho_out != nullptr) write_face_rho<Q>(a.g, a.face_rho_out, x, y, z, rho);
+  if (a.obs_f != nullptr) {
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      a.obs_f[(long long)i * a.g.n + idx] = f[i];
+    });
+  }
+  if (a.obs_rho != nullptr) a.obs_rho[idx] = rho;
+  if (a.obs_u != nullptr) {
+    a.obs_u[3ull * idx] = ux;
+    a.obs_u[3ull * idx + 1] = uy;
+    a.obs_u[3ull * idx + 2] = uz;
+  }
+  if (a.fb != nullptr) collide<Q>(f, a.g, rho, ux, uy, uz);
+}
+
+// One node per thread, nodes in memory order so that each warp owns one
+// 32-node chunk.  Interior nodes pull with constant offsets; face nodes take
+// the face rules.  FORCE adds cul_equ2 and the second moment pass; without it
+// both are exact no-ops (the reference adds zeros and recomputes identical
+// moments), so they are skipped.
+template <int Q, int S, bool FORCE>
+__global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= (unsigned)a.g.n) return;
+  int x, y, z;
+  a.dec(idx, x, y, z);
+  const bool face = on_any_face(a.g, x, y, z);
+  const T *__restrict__ fa = static_cast<const T *>(a.fa);
+  float f[Q];
+  if (!face)
+    pull_interior<Q, S>(fa, a.g, idx, f);
+  else
+    pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
+  finish_node<Q, FORCE>(a, f, idx, x, y, z, face);
+  if (a.fb != nullptr) {
+    T *__restrict__ fb = static_cast<T *>(a.fb);
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      St::store(fb + (long long)i * a.g.n + idx, f[i], V::w(i));
+    });
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Vectorised fused step: thread = NZ consecutive nodes of one z-row (nz a
+// multiple of NZ), populations moved as NZ-element vectors (16 / 8 byte
+// loads and stores).  For rows whose (x, y) is interior every source of
+// direction i lies in row (x - ex, y - ey): one aligned vector load gives
+// NZ - |ez| of the NZ values, one scalar load the remaining one -- from the
+// neighbouring vector, or at z = 0 / z = nz - 1 from the bottom / top face
+// rule.  Rows on an x / y face take the per-node face rules.
+// ---------------------------------------------------------------------------
+template <int Q, int S, int NZ>
+__device__ __forceinline__ float zface_value(const typename Storage<S>::T *__restrict__ fa,
+                                             const Geom &g, int i, int rev, float w, long long row,
+                                             int fc, int x, int y, int z,
+                                             const float *__restrict__ face_rho, float eu) {
+  const int code = g.face[fc];
+  if (code == LBM_BC_PERIODICAL) {
+    // z moved to the opposite plane, same x and y
+    const int zs = (fc == 4) ? g.nz - 1 : 0;
+    return Storage<S>::load(fa + (long long)i * g.n + row + zs, w);
+  }
+  float v = Storage<S>::load(fa + (long long)rev * g.n + row + z, w);
+  if (code == LBM_BC_WALL_WITH_SPEED)
+    v -= 2.f * (face_rho[plane_index(g, fc, x, y, z)] * w) * eu * g.inv_cs2;
+  return v;
+}
+
+template <int Q, int S, bool FORCE, int NZ, int TB>
+__global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  constexpr int kWords = NZ * St::kBits / 32;
+  const unsigned t = blockIdx.x * TB + threadIdx.x;
+  const unsigned idx0 = t * NZ;
+  if (idx0 >= (unsigned)a.g.n) return;
+  int x, y, z0;
+  a.dec(idx0, x, y, z0);
+  const T *__restrict__ fa = static_cast<const T *>(a.fa);
+  const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
+  float f[NZ][Q];
+  if (row_in) {
+    const long long row = (long long)idx0 - z0;
+    const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int ex = V::ex(i), ey = V::ey(i), ez = V::ez(i);
+      constexpr float w = V::w(i);
+      const long long src = (long long)i * a.g.n + idx0 - ((long long)ex * a.g.nyz + (long long)ey * a.g.nz);
+      const Words<kWords> raw = ld_words<kWords>(fa + src);
+      float v[NZ];
+      if constexpr (St::kBits == 32) {
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) v[k] = __uint_as_float(raw.w[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < NZ / 2; ++k) {
+          const float2 p2 = unpack2<S>(raw.w[k], w);
+          v[2 * k] = p2.x;
+          v[2 * k + 1] = p2.y;
+        }
+      }
+      if (ez == 0) {
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) f[k][i] = v[k];
+      } else if (ez > 0) {
+#pragma unroll
+        for (int k = 1; k < NZ; ++k) f[k][i] = v[k - 1];
+        if (bottom) {
+          const float eu = (float)ex * a.g.uw[4][0] + (float)ey * a.g.uw[4][1] + (float)ez * a.g.uw[4][2];
+          f[0][i] = zface_value<Q, S, NZ>(fa, a.g, i, V::rev(i), w, row, 4, x, y, 0, a.face_rho_in, eu);
+        } else {
+          f[0][i] = St::load(fa + src - 1, w);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < NZ - 1; ++k) f[k][i] = v[k + 1];
+        if (top) {
+          const float eu = (float)ex * a.g.uw[5][0] + (float)ey * a.g.uw[5][1] + (float)ez * a.g.uw[5][2];
+          f[NZ - 1][i] = zface_value<Q, S, NZ>(fa, a.g, i, V::rev(i), w, row, 5, x, y, a.g.nz - 1,
+                                               a.face_rho_in, eu);
+        } else {
+          f[NZ - 1][i] = St::load(fa + src + NZ, w);
+        }
+      }
+    });
+  } else {
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) pull_general<Q, S>(fa, a.g, x, y, z0 + k, a.face_rho_in, f[k]);
+  }
+
+#pragma unroll
+  for (int k = 0; k < NZ; ++k) {
+    const int z = z0 + k;
+    finish_node<Q, FORCE>(a, f[k], idx0 + k, x, y, z, !row_in || z == 0 || z == a.g.nz - 1);
+  }
+  if (a.fb == nullptr) return;
+  T *__restrict__ fb = static_cast<T *>(a.fb);
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr float w = V::w(i);
+    Words<kWords> raw;
+    if constexpr (St::kBits == 32) {
+#pragma unroll
+      for (int k = 0; k < NZ; ++k) raw.w[k] = __float_as_uint(f[k][i]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NZ / 2; ++k) raw.w[k] = pack2<S>(f[2 * k][i], f[2 * k + 1][i], w);
+    }
+    st_words(fb + (long long)i * a.g.n + idx0, raw);
+  });
+}
+
+// ---------------------------------------------------------------------------
+// TMA-staged persistent step.  Each CTA walks groups of R whole z-rows
+// (row = (x, y)); for a row with interior (x, y) the source of direction i is
+// row (x - ex, y - ey) of plane i, so one elected thread brings the group in
+// with Q * R bulk copies (cp.async.bulk, completion counted on an mbarrier)
+// into a ring of `stages` shared-memory stages, several groups ahead of the
+// compute.  Threads then read their two consecutive nodes per direction from
+// shared memory (z-1 / z+1 neighbours included; z = 0 / nz - 1 take the
+// bottom / top face rule from global memory), finish the nodes and store
+// them as 8-byte (fp32) / 4-byte (16-bit) pairs.  Rows on an x / y face are
+// pulled from global memory with the full face rules.  Bytes in flight are
+// bounded by shared memory, not registers -- what the 16-bit storage needs
+// to reach HBM bandwidth.  Every barrier wait is bounded; a timeout sets
+// LBM_STATUS_WAIT_TIMEOUT and the CTA drains its copies (bounded) and stops.
+// ---------------------------------------------------------------------------
+constexpr int kTmaThreads = 256;
+constexpr unsigned kTmaWaitPolls = 1u << 24;
+
+struct TmaPlan {
+  int rows_per_stage;
+  int stages;
+  unsigned row_bytes;
+  long long groups;
+};
+
+template <int S>
+__device__ __forceinline__ float sm_elem(const typename Storage<S>::T *p, float w) {
+  if constexpr (Storage<S>::kBits == 32)
+    return *p;
+  else if constexpr (S == LBM_STORAGE_FP16S)
+    return w + __half2float(*p);
+  else
+    return w + __bfloat162float(*p);
+}
+
+template <int S>
+__device__ __forceinline__ float2 sm_pair(const typename Storage<S>::T *p, float w) {
+  if constexpr (Storage<S>::kBits == 32)
+    return *reinterpret_cast<const float2 *>(p);
+  else
+    return unpack2<S>(*reinterpret_cast<const unsigned *>(p), w);
+}
+
+template <int Q, int S, bool FORCE>
+__global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, const TmaPlan p) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  T *buf = reinterpret_cast<T *>(smem + 128);
+  const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
+  const int R = p.rows_per_stage;
+  const T *__restrict__ fa = static_cast<const T *>(a.fa);
+  const int tid = threadIdx.x;
+  const long long G = gridDim.x;
+  if (tid == 0) {
+    for (int s = 0; s < p.stages; ++s) mbar_init(&bars[s], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  auto row_xy = [&](long long r, int &x, int &y) {
+    x = (int)(r / ny);
+    y = (int)(r - (long long)x * ny);
+  };
+  auto interior = [&](int x, int y) { return x > 0 && x < nx - 1 && y > 0 && y < ny - 1; };
+  auto issue = [&](int s, long long g) {
+    const long long r0 = g * R;
+    unsigned bytes = 0;
+    for (int j = 0; j < R; ++j) {
+      int x, y;
+      row_xy(r0 + j, x, y);
+      if (interior(x, y)) bytes += Q * p.row_bytes;
+    }
+    if (bytes == 0) {
+      mbar_arrive(&bars[s]);
+      return;
+    }
+    mbar_arrive_expect_tx(&bars[s], bytes);
+    for (int j = 0; j < R; ++j) {
+      int x, y;
+      row_xy(r0 + j, x, y);
+      if (!interior(x, y)) continue;
+      T *dst = buf + (long long)(s * R + j) * Q * nz;
+      static_for<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const T *src = fa + (long long)i * a.g.n +
+                       ((long long)(x - V::ex(i)) * ny + (y - V::ey(i))) * nz;
+        bulk_copy_g2s(dst + (long long)i * nz, src, p.row_bytes, &bars[s]);
+      });
+    }
+  };
+  if (tid == 0) {
+    for (int s = 0; s < p.stages; ++s) {
+      const long long g = blockIdx.x + s * G;
+      if (g < p.groups) issue(s, g);
+    }
+  }
+
+  const int half = nz / 2;
+  long long k = 0;
+  bool timed_out = false;
+  for (;; ++k) {
+    const long long g = blockIdx.x + k * G;
+    if (g >= p.groups) break;
+    const int s = (int)(k % p.stages);
+    const unsigned par = (unsigned)((k / p.stages) & 1);
+    const bool ok = mbar_wait_bounded(&bars[s], par, kTmaWaitPolls);
+    if (__syncthreads_or(!ok)) {
+      timed_out = true;
+      break;
+    }
+    for (int pi = tid; pi < R * half; pi += kTmaThreads) {
+      const int j = pi / half, zp = pi - j * half;
+      const long long r = g * R + j;
+      int x, y;
+      row_xy(r, x, y);
+      const int z = 2 * zp;
+      const unsigned idx = (unsigned)(r * nz + z);
+      float f0[Q], f1[Q];
+      const bool row_in = interior(x, y);
+      if (row_in) {
+        const T *srow = buf + (long long)(s * R + j) * Q * nz;
+        const long long row = r * nz;
+        static_for<Q>([&](auto ic) {
+          constexpr int i = decltype(ic)::value;
+          constexpr int ez = V::ez(i);
+          constexpr float w = V::w(i);
+          const T *rp = srow + (long long)i * nz;
+          if constexpr (ez == 0) {
+            const float2 v = sm_pair<S>(rp + z, w);
+            f0[i] = v.x;
+            f1[i] = v.y;
+          } else if constexpr (ez > 0) {
+            f1[i] = sm_elem<S>(rp + z, w);
+            if (z == 0) {
+              const float eu = (float)V::ex(i) * a.g.uw[4][0] + (float)V::ey(i) * a.g.uw[4][1] +
+                               (float)ez * a.g.uw[4][2];
+              f0[i] = zface_value<Q, S, 2>(fa, a.g, i, V::rev(i), w, row, 4, x, y, 0,
+                                           a.face_rho_in, eu);
+            } else {
+              f0[i] = sm_elem<S>(rp + z - 1, w);
+            }
+          } else {
+            f0[i] = sm_elem<S>(rp + z + 1, w);
+            if (z + 2 == nz) {
+              const float eu = (float)V::ex(i) * a.g.uw[5][0] + (float)V::ey(i) * a.g.uw[5][1] +
+                               (float)ez * a.g.uw[5][2];
+              f1[i] = zface_value<Q, S, 2>(fa, a.g, i, V::rev(i), w, row, 5, x, y, nz - 1,
+                                           a.face_rho_in, eu);
+            } else {
+              f1[i] = sm_elem<S>(rp + z + 2, w);
+            }
+          }
+        });
+      } else {
+        pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f0);
+        pull_general<Q, S>(fa, a.g, x, y, z + 1, a.face_rho_in, f1);
+      }
+      finish_node<Q, FORCE>(a, f0, idx, x, y, z, !row_in || z == 0);
+      finish_node<Q, FORCE>(a, f1, idx + 1, x, y, z + 1, !row_in || z + 1 == nz - 1);
+      if (a.fb != nullptr) {
+        T *__restrict__ fb = static_cast<T *>(a.fb);
+        static_for<Q>([&](auto ic) {
+          constexpr int i = decltype(ic)::value;
+          constexpr float w = V::w(i);
+          T *dst = fb + (long long)i * a.g.n + idx;
+          if constexpr (St::kBits == 32)
+            *reinterpret_cast<float2 *>(dst) = make_float2(f0[i], f1[i]);
+          else
+            *reinterpret_cast<unsigned *>(dst) = pack2<S>(f0[i], f1[i], w);
+        });
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const long long g2 = g + (long long)p.stages * G;
+      if (g2 < p.groups) {
+        fence_proxy_async_smem();
+        issue(s, g2);
+      }
+    }
+  }
+  if (timed_out && tid == 0) {
+    if (a.status != nullptr) atomicOr(a.status, LBM_STATUS_WAIT_TIMEOUT);
+    // drain the copies still in flight into this CTA's shared memory
+    for (long long kk = k; kk < k + p.stages; ++kk) {
+      if (blockIdx.x + kk * G >= p.groups) break;
+      mbar_wait_bounded(&bars[kk % p.stages], (unsigned)((kk / p.stages) & 1), kTmaWaitPolls);
+    }
+  }
+}
+
+// Launch shape of the fused step: nodes per thread (1 = scalar kernel, or
+// NZ consecutive z-nodes moved as 4 / 8 / 16-byte vectors, nz a multiple of
+// NZ) and threads per block.
+inline bool step_shape_ok(int nodes, int nz, int bits) {
+  if (nodes == 1) return true;
+  if (nodes != 2 && nodes != 4 && nodes != 8) return false;
+  if (nodes * bits / 32 < 1 || nodes * bits / 32 > 4) return false;
+  return nz % nodes == 0 && nz >= 2 * nodes;
+}
+
+// Shared-memory plan of the TMA-staged step for this device, or false when
+// the lattice does not qualify (rows must be a multiple of 16 bytes, the
+// population buffer 16-byte aligned, and two stages must fit).
+struct DeviceInfo {
+  int sms = 0, smem_sm = 0, smem_optin = 0;
+};
+
+inline bool device_info(DeviceInfo &d) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&d.smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+      cudaSuccess)
+    return false;
+  if (cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+      cudaSuccess)
+    return false;
+  return true;
+}
+
+inline bool tma_plan(const Geom &g, int q, int bits, const void *fa, TmaPlan &p, int &ctas,
+                     size_t &smem, unsigned &grid) {
+  const int elem = bits / 8;
+  const long long row_bytes = (long long)g.nz * elem;
+  if (row_bytes % 16 != 0 || g.nz < 16 || ((uintptr_t)fa & 15u) != 0) return false;
+  DeviceInfo d;
+  if (!device_info(d)) return false;
+  const long long rows = (long long)g.nx * g.ny;
+  int R = 2 * kTmaThreads / g.nz;
+  if (R < 1 || rows % R != 0) R = 1;
+  const long long stage = (long long)R * q * row_bytes;
+  const long long reserve = 1024 + 128;
+  int stages = (int)std::min<long long>(8, (d.smem_sm / 2 - reserve) / stage);
+  ctas = 2;
+  if (stages < 3) {
+    ctas = 1;
+    stages = (int)std::min<long long>(8, (std::min(d.smem_optin, d.smem_sm) - reserve) / stage);
+  }
+  if (stages < 2) return false;
+  p.rows_per_stage = R;
+  p.stages = stages;
+  p.row_bytes = (unsigned)row_bytes;
+  p.groups = rows / R;
+  smem = 128 + (size_t)stages * stage;
+  const long long want = (long long)ctas * d.sms;
+  grid = (unsigned)std::min<long long>(p.groups, want);
+  return true;
+}
+
+template <int Q, int S>
+struct StepLauncher {
+  template <bool FORCE>
+  static int go_tma_f(const StepArgs &a, cudaStream_t s) {
+    TmaPlan p;
+    int ctas;
+    size_t smem;
+    unsigned grid;
+    if (!tma_plan(a.g, Q, Storage<S>::kBits, a.fa, p, ctas, smem, grid)) {
+      set_error("lbm_flow_step: this lattice does not qualify for row staging (rows must be a "
+                "multiple of 16 bytes and at least 16 nodes, buffers 16-byte aligned)");
+      return LBM_ERR_INVALID;
+    }
+    cudaError_t e = cudaFuncSetAttribute(k_step_tma<Q, S, FORCE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail_cuda(e, "lbm_flow_step");
+    k_step_tma<Q, S, FORCE><<<grid, kTmaThreads, smem, s>>>(a, p);
+    return LBM_OK;
+  }
+  static int go_tma(const StepArgs &a, bool force, cudaStream_t s) {
+    return force ? go_tma_f<true>(a, s) : go_tma_f<false>(a, s);
+  }
+
+  template <int NZ, int TB>
+  static void go_vec(const StepArgs &a, bool force, cudaStream_t s) {
+    const unsigned nb = blocks_for(a.g.n / NZ, TB);
+    if (force)
+      k_step_vec<Q, S, true, NZ, TB><<<nb, TB, 0, s>>>(a);
+    else
+      k_step_vec<Q, S, false, NZ, TB><<<nb, TB, 0, s>>>(a);
+  }
+  template <int NZ>
+  static void go_nz(const StepArgs &a, bool force, int threads, cudaStream_t s) {
+    if (threads == 128)
+      go_vec<NZ, 128>(a, force, s);
+    else
+      go_vec<NZ, 256>(a, force, s);
+  }
+  static int go(const StepArgs &a, bool force, int nodes, int threads, cudaStream_t s) {
+    constexpr int bits = Storage<S>::kBits;
+    if (nodes == LBM_STEP_ROWS) return go_tma(a, force, s);
+    if (nodes == 0) {
+      // measured on B200: 2 nodes per thread with 128-thread blocks is the
+      // fastest shape for every velocity set in float32 (see funlbm_b200.tune)
+      nodes = step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
+      threads = threads ? threads : 128;
+    }
+    if (nodes == 2) {
+      go_nz<2>(a, force, threads, s);
+      return LBM_OK;
+    }
+    if (nodes == 4) {
+      go_nz<4>(a, force, threads, s);
+      return LBM_OK;
+    }
+    if constexpr (bits == 16) {
+      if (nodes == 8) {
+        go_nz<8>(a, force, threads, s);
+        return LBM_OK;
+      }
+    }
+    const unsigned nb = blocks_for(a.g.n, kThreads);
+    if (force)
+      k_step<Q, S, true><<<nb, kThreads, 0, s>>>(a);
+    else
+      k_step<Q, S, false><<<nb, kThreads, 0, s>>>(a);
+    return LBM_OK;
+  }
+};
+
+// One fused step for velocity set Q and storage S (explicitly instantiated
+// once per (Q, S) in lbm_step_inst.cu, so the launch-shape variants compile
+// in parallel translation units).
+template <int Q, int S>
+int run_step_qs(const StepArgs &a, bool force, int nodes, int threads, cudaStream_t s) {
+  const int rc = StepLauncher<Q, S>::go(a, force, nodes, threads, s);
+  if (rc) return rc;
+  LBM_LAUNCH_CHECK("lbm_flow_step");
+  return LBM_OK;
+}
+
+#define LBM_FOR_EACH_QS(X) \
+  X(13, 0) X(13, 1) X(13, 2) X(15, 0) X(15, 1) X(15, 2) X(19, 0) X(19, 1) X(19, 2) X(27, 0) \
+  X(27, 1) X(27, 2)
+
+}  // namespace lbm
