@@ -23,6 +23,7 @@ LBM_STATUS_STENCIL_EMPTY = 0x4
 LBM_STATUS_WAIT_TIMEOUT = 0x8
 
 STORAGE = {"fp32": 0, "fp16s": 1, "bf16s": 2}
+SPREAD_NOALLOC_MAX_NODES = 1 << 22
 RIGID_WALL = 1
 RIGID_UPDATE = 2
 
@@ -107,6 +108,7 @@ SIGNATURES = {
     "ibm_interpolate": (I, [_LAT, _P, _FORCE, _P, _P, _P, _PART, F, ctypes.c_int32, _P, _P]),
     "rigid_wall_and_update": (I, [_LAT, _PART, ctypes.c_int32, F, F, F, F, _P]),
     "ibm_spread": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P, _P]),
+    "ibm_spread_noalloc": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P]),
     "rigid_update_markers": (I, [_PART, _P]),
     "lbm_last_error": (ctypes.c_char_p, []),
     "lbm_version": (ctypes.c_char_p, []),

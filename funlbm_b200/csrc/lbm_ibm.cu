@@ -1,6 +1,9 @@
 // Immersed boundary coupling and rigid particles: interpolation (fused with
 // the moment pass it reads), wall spring + Newton-Euler update, spreading,
 // and the rotation-vector marker update.
+#include <algorithm>
+#include <mutex>
+
 #include "lbm_api.cuh"
 
 namespace lbm {
@@ -442,6 +445,48 @@ static int check_particles(const lbm_particles *pt, const char *who) {
   return LBM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Claim array of ibm_spread_noalloc.  It lives in the library's own device
+// memory (one copy per GPU that loads the library, kept until exit), so
+// that entry point needs no buffer from the caller and allocates nothing.
+// Host code must not use the symbol itself -- only the device address that
+// cudaGetSymbolAddress returns for the current device.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) int32_t g_spread_owner[LBM_SPREAD_NOALLOC_MAX_NODES];
+
+__global__ void k_owner_reset(int32_t *owner, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    owner[i] = -1;
+}
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_owner_mu;
+int32_t *g_owner_addr[kMaxDevices] = {};
+}  // namespace
+
+// Device address of g_spread_owner on the current device, looked up once per
+// device (the first call on a device does this set-up).
+static int owner_scratch(int32_t **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail_cuda(e, "ibm_spread_noalloc");
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("ibm_spread_noalloc: device index %d out of range", dev);
+    return LBM_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(g_owner_mu);
+  if (g_owner_addr[dev] == nullptr) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_spread_owner);
+    if (e != cudaSuccess) return fail_cuda(e, "ibm_spread_noalloc: cudaGetSymbolAddress");
+    g_owner_addr[dev] = static_cast<int32_t *>(p);
+  }
+  *out = g_owner_addr[dev];
+  return LBM_OK;
+}
+
 }  // namespace lbm
 
 using namespace lbm;
@@ -573,6 +618,56 @@ int rigid_update_markers(const lbm_particles *pt, void *stream) {
   if (pt->n_particles == 0) return LBM_OK;
   k_markers<<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
   LBM_LAUNCH_CHECK("rigid_update_markers");
+  return LBM_OK;
+}
+
+// Same spreading as ibm_spread, with the per-node claim array taken from the
+// library's static device array instead of from the caller.
+int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
+                       uint8_t *chunks, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if ((rc = check_particles(pt, "ibm_spread_noalloc"))) return rc;
+  if (mode != 0 && mode != 1) {
+    set_error("ibm_spread_noalloc: mode must be 0 (reference) or 1 (accumulate)");
+    return LBM_ERR_INVALID;
+  }
+  if (field == nullptr || chunks == nullptr) {
+    set_error("ibm_spread_noalloc: field and chunks are required");
+    return LBM_ERR_INVALID;
+  }
+  const long long n = (long long)lat->nx * lat->ny * lat->nz;
+  if (n > LBM_SPREAD_NOALLOC_MAX_NODES) {
+    set_error("ibm_spread_noalloc: the lattice has %lld nodes, more than the %d nodes its "
+              "built-in claim array holds; use ibm_spread with a caller-owned array",
+              n, (int)LBM_SPREAD_NOALLOC_MAX_NODES);
+    return LBM_ERR_INVALID;
+  }
+  int32_t *owner = nullptr;
+  if ((rc = owner_scratch(&owner))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the array keeps whatever the previous call left: reset the part used
+  k_owner_reset<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, s>>>(owner, n);
+  LBM_LAUNCH_CHECK("ibm_spread_noalloc");
+  SpreadArgs a;
+  a.g = make_geom(lat);
+  a.p = *pt;
+  a.field = field;
+  a.chunks = chunks;
+  a.owner = owner;
+  const long long nchunks = (a.g.n + 31) >> 5;
+  k_spread_clear<<<blocks_for(nchunks * 32, 256), 256, 0, s>>>(a.g.n, field, chunks);
+  LBM_LAUNCH_CHECK("ibm_spread_noalloc");
+  if (pt->n_markers == 0) return LBM_OK;
+  const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
+  if (mode == 0) {
+    k_spread<0><<<nb, kIbmThreads, 0, s>>>(a);
+    k_spread<1><<<nb, kIbmThreads, 0, s>>>(a);
+    k_spread<2><<<nb, kIbmThreads, 0, s>>>(a);
+  } else {
+    k_spread<3><<<nb, kIbmThreads, 0, s>>>(a);
+  }
+  LBM_LAUNCH_CHECK("ibm_spread_noalloc");
   return LBM_OK;
 }
 

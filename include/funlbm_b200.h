@@ -209,6 +209,24 @@ int rigid_wall_and_update(const lbm_lattice *lat, const lbm_particles *pt, int32
 int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
                uint8_t *chunks, int32_t *owner, void *stream);
 
+/* Allocation-free ibm_spread.  No counterpart in the reference.  For callers
+ * that cannot allocate device memory themselves -- a host program that only
+ * has the lattice's own buffers (a solver coupled in through this C ABI from
+ * another language, or a loop with a fixed device-memory budget where a
+ * cudaMalloc would fail or synchronise the device) -- the per-node claim
+ * array that ibm_spread takes from the caller is here a static array inside
+ * the library: LBM_SPREAD_NOALLOC_MAX_NODES int32 (16 MiB), held on every GPU
+ * that loads the library until the process exits.  Lattices with more nodes
+ * are rejected with LBM_ERR_INVALID.  The call allocates nothing.  Its first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the one array and each resets
+ * the part it uses: calls whose work overlaps on the GPU race, so issue them
+ * in order on one stream.  Arguments and results are those of ibm_spread
+ * without `owner`. */
+#define LBM_SPREAD_NOALLOC_MAX_NODES (1 << 22)
+int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
+                       uint8_t *chunks, void *stream);
+
 /* Particle.update + Coordinate.update/cul_point (particle/base/base.py:153-156,
  * particle/coord.py:87-108): angle += cw; lx = R(angle) lagrange + cx, with the
  * rotation built in float64 from the rotation vector. */
