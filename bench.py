@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-size", type=int, default=64)
+    ap.add_argument("--shape", default=None,
+                    help="fixed launch shape 'nodes,threads' (e.g. 2,128 or -1,256) instead of "
+                         "the autotuner")
     return ap.parse_args()
 
 
@@ -185,7 +188,11 @@ def run_device(args, world, rank, local):
     f0 = taylor_green_soa(lat, torch)
     lat.init(f0)
     del f0
-    shape, _ = lat.tune()          # launch-shape autotuner (scratch proxy lattice)
+    if args.shape:
+        shape = tuple(int(v) for v in args.shape.split(","))
+        lat.set_launch_shape(*shape)
+    else:
+        shape, _ = lat.tune()      # launch-shape autotuner (scratch proxy lattice)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         lat.step(None)
