@@ -5,8 +5,10 @@
 
 namespace lbm {
 
-#define LBM_EXTERN_STEP(Q, S) \
-  extern template int run_step_qs<Q, S>(const StepArgs &, bool, int, int, cudaStream_t);
+#define LBM_EXTERN_STEP(Q, S)                                                                 \
+  extern template int run_step_qs<Q, S>(const StepArgs &, bool, int, int, cudaStream_t);      \
+  extern template int run_step_batch_qs<Q, S>(const StepArgs *, const unsigned *, int, unsigned, \
+                                              bool, int, cudaStream_t);
 LBM_FOR_EACH_QS(LBM_EXTERN_STEP)
 #undef LBM_EXTERN_STEP
 
@@ -274,6 +276,55 @@ struct RunForce {
   }
 };
 
+// StepArgs of one fused step (shared by lbm_flow_step and lbm_batch_pack).
+static int build_step_args(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
+                           const float *face_rho_in, float *face_rho_out, const lbm_observe *obs,
+                           uint32_t *status, StepArgs &a, bool &use_force, const char *who) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if (any_face(lat, LBM_BC_NON_EQUILIBRIUM)) {
+    set_error("%s: NON_EQUILIBRIUM faces need the global inlet density; run them "
+              "through lbm_collide / lbm_stream / lbm_moments / lbm_add_force", who);
+    return LBM_ERR_UNSUPPORTED;
+  }
+  if (fa == nullptr) {
+    set_error("%s: input populations are NULL", who);
+    return LBM_ERR_INVALID;
+  }
+  const bool wws = any_face(lat, LBM_BC_WALL_WITH_SPEED);
+  if (wws && face_rho_in == nullptr) {
+    set_error("%s: WALL_WITH_SPEED faces need face_rho_in", who);
+    return LBM_ERR_INVALID;
+  }
+  memset(&a, 0, sizeof(a));
+  a.g = make_geom(lat);
+  a.dec = make_decomp(a.g);
+  a.fa = fa;
+  a.fb = fb;
+  use_force = false;
+  if (force != nullptr) {
+    for (int k = 0; k < 3; ++k) {
+      a.go[k] = force->old_uniform[k];
+      a.gn[k] = force->new_uniform[k];
+      use_force = use_force || a.go[k] != 0.f || a.gn[k] != 0.f;
+    }
+    a.fol_old = force->old_field;
+    a.fol_new = force->new_field;
+    a.ch_old = force->old_chunks;
+    a.ch_new = force->new_chunks;
+    use_force = use_force || a.fol_old != nullptr || a.fol_new != nullptr;
+  }
+  a.face_rho_in = face_rho_in;
+  a.face_rho_out = wws ? face_rho_out : nullptr;
+  if (obs != nullptr) {
+    a.obs_f = obs->f;
+    a.obs_rho = obs->rho;
+    a.obs_u = obs->u;
+  }
+  a.status = status;
+  return LBM_OK;
+}
+
 }  // namespace lbm
 
 using namespace lbm;
@@ -300,49 +351,11 @@ int lbm_flow_init(const lbm_lattice *lat, const float *f0, void *fa, float *face
 int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
                   const float *face_rho_in, float *face_rho_out, const lbm_observe *obs,
                   uint32_t *status, void *stream) {
-  int rc = check_lattice(lat);
-  if (rc) return rc;
-  if (any_face(lat, LBM_BC_NON_EQUILIBRIUM)) {
-    set_error("lbm_flow_step: NON_EQUILIBRIUM faces need the global inlet density; run them "
-              "through lbm_collide / lbm_stream / lbm_moments / lbm_force");
-    return LBM_ERR_UNSUPPORTED;
-  }
-  if (fa == nullptr) {
-    set_error("lbm_flow_step: input populations are NULL");
-    return LBM_ERR_INVALID;
-  }
-  const bool wws = any_face(lat, LBM_BC_WALL_WITH_SPEED);
-  if (wws && face_rho_in == nullptr) {
-    set_error("lbm_flow_step: WALL_WITH_SPEED faces need face_rho_in");
-    return LBM_ERR_INVALID;
-  }
   StepArgs a;
-  memset(&a, 0, sizeof(a));
-  a.g = make_geom(lat);
-  a.dec = make_decomp(a.g);
-  a.fa = fa;
-  a.fb = fb;
   bool use_force = false;
-  if (force != nullptr) {
-    for (int k = 0; k < 3; ++k) {
-      a.go[k] = force->old_uniform[k];
-      a.gn[k] = force->new_uniform[k];
-      use_force = use_force || a.go[k] != 0.f || a.gn[k] != 0.f;
-    }
-    a.fol_old = force->old_field;
-    a.fol_new = force->new_field;
-    a.ch_old = force->old_chunks;
-    a.ch_new = force->new_chunks;
-    use_force = use_force || a.fol_old != nullptr || a.fol_new != nullptr;
-  }
-  a.face_rho_in = face_rho_in;
-  a.face_rho_out = wws ? face_rho_out : nullptr;
-  if (obs != nullptr) {
-    a.obs_f = obs->f;
-    a.obs_rho = obs->rho;
-    a.obs_u = obs->u;
-  }
-  a.status = status;
+  int rc = build_step_args(lat, fa, fb, force, face_rho_in, face_rho_out, obs, status, a,
+                           use_force, "lbm_flow_step");
+  if (rc) return rc;
   const int bits = lat->storage == LBM_STORAGE_FP32 ? 32 : 16;
   if (lat->step_nodes != 0 && lat->step_nodes != LBM_STEP_ROWS &&
       !step_shape_ok(lat->step_nodes, lat->nz, bits)) {
@@ -356,6 +369,59 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
   }
   return run_step(a, lat->q, lat->storage, use_force, (int)lat->step_nodes,
                   (int)lat->step_threads, (cudaStream_t)stream);
+}
+
+size_t lbm_batch_entry_bytes(void) { return sizeof(StepArgs); }
+
+int lbm_batch_pack(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
+                   const float *face_rho_in, float *face_rho_out, uint32_t *status, int32_t nodes,
+                   void *entry, uint32_t *blocks) {
+  if (entry == nullptr || blocks == nullptr) {
+    set_error("lbm_batch_pack: entry and blocks are required");
+    return LBM_ERR_INVALID;
+  }
+  if (fb == nullptr) {
+    set_error("lbm_batch_pack: a batched step needs an output buffer");
+    return LBM_ERR_INVALID;
+  }
+  StepArgs a;
+  bool use_force = false;
+  int rc = build_step_args(lat, fa, fb, force, face_rho_in, face_rho_out, nullptr, status, a,
+                           use_force, "lbm_batch_pack");
+  if (rc) return rc;
+  const int bits = lat->storage == LBM_STORAGE_FP32 ? 32 : 16;
+  if (nodes != 1 && !(nodes == 2 && step_shape_ok(2, lat->nz, bits))) {
+    set_error("lbm_batch_pack: nodes per thread must be 1, or 2 for rows of an even number "
+              "(>= 4) of nodes");
+    return LBM_ERR_INVALID;
+  }
+  const long long threads = nodes == 2 ? 128 : 256;
+  const long long work = a.g.n / nodes;
+  *blocks = (uint32_t)((work + threads - 1) / threads);
+  memcpy(entry, &a, sizeof(a));
+  return LBM_OK;
+}
+
+int lbm_flow_step_batch(int32_t q, int32_t storage, int32_t nodes, int32_t force,
+                        const void *entries, const uint32_t *block_begin, int32_t count,
+                        uint32_t total_blocks, void *stream) {
+  if (entries == nullptr || block_begin == nullptr || count <= 0 || total_blocks == 0) {
+    set_error("lbm_flow_step_batch: empty batch");
+    return LBM_ERR_INVALID;
+  }
+  if (nodes != 1 && nodes != 2) {
+    set_error("lbm_flow_step_batch: nodes per thread must be 1 or 2");
+    return LBM_ERR_INVALID;
+  }
+  const StepArgs *e = static_cast<const StepArgs *>(entries);
+  cudaStream_t s = (cudaStream_t)stream;
+#define LBM_CASE_BATCH(Q, S)                                                             \
+  if (q == Q && storage == S)                                                            \
+    return run_step_batch_qs<Q, S>(e, block_begin, count, total_blocks, force != 0, nodes, s);
+  LBM_FOR_EACH_QS(LBM_CASE_BATCH)
+#undef LBM_CASE_BATCH
+  set_error("lbm_flow_step_batch: unknown velocity set D3Q%d or storage %d", q, storage);
+  return LBM_ERR_INVALID;
 }
 
 int lbm_collide(const lbm_lattice *lat, float *f, const float *rho, const float *u, float *feq,

@@ -87,11 +87,10 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsig
 // both are exact no-ops (the reference adds zeros and recomputes identical
 // moments), so they are skipped.
 template <int Q, int S, bool FORCE>
-__global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
+__device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsigned idx) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
-  const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= (unsigned)a.g.n) return;
   int x, y, z;
   a.dec(idx, x, y, z);
@@ -110,6 +109,11 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
       St::store(fb + (long long)i * a.g.n + idx, f[i], V::w(i));
     });
   }
+}
+
+template <int Q, int S, bool FORCE>
+__global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
+  step_scalar_body<Q, S, FORCE>(a, blockIdx.x * kThreads + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -138,13 +142,12 @@ __device__ __forceinline__ float zface_value(const typename Storage<S>::T *__res
   return v;
 }
 
-template <int Q, int S, bool FORCE, int NZ, int TB>
-__global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
+template <int Q, int S, bool FORCE, int NZ>
+__device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned t) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
   constexpr int kWords = NZ * St::kBits / 32;
-  const unsigned t = blockIdx.x * TB + threadIdx.x;
   const unsigned idx0 = t * NZ;
   if (idx0 >= (unsigned)a.g.n) return;
   int x, y, z0;
@@ -222,6 +225,52 @@ __global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
     }
     st_words(fb + (long long)i * a.g.n + idx0, raw);
   });
+}
+
+template <int Q, int S, bool FORCE, int NZ, int TB>
+__global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
+  step_vec_body<Q, S, FORCE, NZ>(a, blockIdx.x * TB + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-lattice step: one launch advances `count` independent lattices of one
+// velocity set and storage by one step.  Lattice e owns blocks
+// [block_begin[e], block_begin[e+1]); each block finds its lattice by binary
+// search, copies that lattice's StepArgs into shared memory and runs the
+// same per-node code as the single-lattice kernels (NZ = 1: k_step's body,
+// NZ > 1: k_step_vec's), so a lattice's result does not depend on which
+// other lattices share the launch.
+// ---------------------------------------------------------------------------
+template <int Q, int S, bool FORCE, int NZ, int TB>
+__global__ void __launch_bounds__(TB)
+    k_step_batch(const StepArgs *__restrict__ entries, const unsigned *__restrict__ block_begin,
+                 int count) {
+  __shared__ __align__(16) StepArgs sa;
+  __shared__ unsigned s_entry;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (block_begin[mid] <= blockIdx.x)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    s_entry = (unsigned)lo;
+  }
+  __syncthreads();
+  const unsigned e = s_entry;
+  constexpr int kWordsArgs = (int)(sizeof(StepArgs) / 4);
+  static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied as 32-bit words");
+  const unsigned *src = reinterpret_cast<const unsigned *>(entries + e);
+  unsigned *dst = reinterpret_cast<unsigned *>(&sa);
+  for (int w = threadIdx.x; w < kWordsArgs; w += TB) dst[w] = src[w];
+  __syncthreads();
+  const unsigned t = (blockIdx.x - block_begin[e]) * TB + threadIdx.x;
+  if constexpr (NZ == 1)
+    step_scalar_body<Q, S, FORCE>(sa, t);
+  else
+    step_vec_body<Q, S, FORCE, NZ>(sa, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -546,6 +595,26 @@ struct StepLauncher {
     return LBM_OK;
   }
 };
+
+// Multi-lattice launch for velocity set Q and storage S: nodes per thread 1
+// (256 threads) or 2 (128 threads).
+template <int Q, int S>
+int run_step_batch_qs(const StepArgs *entries, const unsigned *block_begin, int count,
+                      unsigned total_blocks, bool force, int nodes, cudaStream_t s) {
+  if (nodes == 2) {
+    if (force)
+      k_step_batch<Q, S, true, 2, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
+    else
+      k_step_batch<Q, S, false, 2, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
+  } else {
+    if (force)
+      k_step_batch<Q, S, true, 1, 256><<<total_blocks, 256, 0, s>>>(entries, block_begin, count);
+    else
+      k_step_batch<Q, S, false, 1, 256><<<total_blocks, 256, 0, s>>>(entries, block_begin, count);
+  }
+  LBM_LAUNCH_CHECK("lbm_flow_step_batch");
+  return LBM_OK;
+}
 
 // One fused step for velocity set Q and storage S (explicitly instantiated
 // once per (Q, S) in lbm_step_inst.cu, so the launch-shape variants compile

@@ -285,6 +285,14 @@ class FlowD3(Flow):
         self._keep = keep
         self._obs_valid = False
 
+    def stepped_elsewhere(self, force, new_field=None, new_uniform=(0.0, 0.0, 0.0), keep=()):
+        """Record a fused step whose kernel ran in a multi-lattice launch
+        (the populations moved from buf[cur] to buf[cur ^ 1])."""
+        self._lat.cur ^= 1
+        self._last_force = (force, (new_field, tuple(new_uniform)))
+        self._keep = keep
+        self._obs_valid = False
+
     def read_status(self):
         return self._lat.read_status() if self._lat is not None and self._lat.status is not None else 0
 

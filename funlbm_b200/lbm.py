@@ -318,6 +318,17 @@ class LBMD3(LBMBase):
 
     # -- fused step ---------------------------------------------------------------
     def _fused_step(self):
+        plan = self.fused_prepare()
+        self.flow.fused_step(plan["force"], plan["new_field"], plan["g_new"], keep=plan["keep"])
+        self.fused_finish(plan)
+
+    def fused_prepare(self, launch=True):
+        """Everything of a fused step that precedes the step kernel: enter the
+        fused representation, and with particles interpolate, apply the wall
+        spring and the Newton-Euler update and spread the marker forces.
+        Returns the step's force description for the step kernel (run here by
+        ``_fused_step``, or packed with other lattices by a server).  With
+        launch=False only the description is computed (nothing is issued)."""
         fl = self.flow
         entering = fl._mode != "fused"
         fl.enter_fused()
@@ -329,32 +340,41 @@ class LBMD3(LBMBase):
             self._ensure_ibm()
         if self._fol is None:
             force = None if (g_new == (0, 0, 0) and g_old == (0, 0, 0)) else make_force(g_old, g_new)
-            fl.fused_step(force, None, g_new)
-        else:
-            s = self._stream()
-            new, old = self._fi, self._fi ^ 1
-            F_new, F_old = self._fol[new], self._fol[old]
-            C_new, C_old = self._chunks[new], self._chunks[old]
-            if parts:
-                sw = self.particle_swarm
-                st = ctypes.byref(sw.struct())
-                f_int = make_force(old_uniform=g_old, old_field=F_old)
-                call("ibm_interpolate", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]), ctypes_ref(f_int),
-                     ptr(lat.face_rho[lat.cur]), None, None, st, float(self.config.dt),
-                     int(self.step), ptr(self._status_ibm), s)
-                call("rigid_wall_and_update", ctypes_ref(lat.desc), st,
-                     _lib.RIGID_WALL | _lib.RIGID_UPDATE, float(self.config.dt),
-                     float(self.config.dx), float(self.config.flow_config.gl), 1.0, s)
-            mode = 0 if self.config.ibm_mode == "reference" else 1
-            sw_struct = self.particle_swarm.struct() if parts else _empty_particles()
-            call("ibm_spread", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode, ptr(F_new),
-                 ptr(C_new), ptr(self._owner), s)
-            force = make_force(g_old, g_new, F_old, F_new, C_old, C_new)
-            fl.fused_step(force, F_new, g_new, keep=(F_old, F_new, C_old, C_new))
-            if parts:
-                call("rigid_update_markers", ctypes.byref(self.particle_swarm.struct()), s)
+            return {"force": force, "new_field": None, "g_new": g_new, "keep": (), "ibm": False}
+        s = self._stream()
+        new, old = self._fi, self._fi ^ 1
+        F_new, F_old = self._fol[new], self._fol[old]
+        C_new, C_old = self._chunks[new], self._chunks[old]
+        force = make_force(g_old, g_new, F_old, F_new, C_old, C_new)
+        plan = {"force": force, "new_field": F_new, "g_new": g_new,
+                "keep": (F_old, F_new, C_old, C_new), "ibm": True}
+        if not launch:
+            return plan
+        if parts:
+            sw = self.particle_swarm
+            st = ctypes.byref(sw.struct())
+            f_int = make_force(old_uniform=g_old, old_field=F_old)
+            call("ibm_interpolate", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]), ctypes_ref(f_int),
+                 ptr(lat.face_rho[lat.cur]), None, None, st, float(self.config.dt),
+                 int(self.step), ptr(self._status_ibm), s)
+            call("rigid_wall_and_update", ctypes_ref(lat.desc), st,
+                 _lib.RIGID_WALL | _lib.RIGID_UPDATE, float(self.config.dt),
+                 float(self.config.dx), float(self.config.flow_config.gl), 1.0, s)
+        mode = 0 if self.config.ibm_mode == "reference" else 1
+        sw_struct = self.particle_swarm.struct() if parts else _empty_particles()
+        call("ibm_spread", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode, ptr(F_new),
+             ptr(C_new), ptr(self._owner), s)
+        return plan
+
+    def fused_finish(self, plan):
+        """Everything of a fused step after the step kernel: the marker update
+        and the force-buffer swap."""
+        if plan["ibm"]:
+            if self.particle_swarm.particles:
+                call("rigid_update_markers", ctypes.byref(self.particle_swarm.struct()),
+                     self._stream())
             self._fi ^= 1
-        self._g_old = g_new
+        self._g_old = plan["g_new"]
 
     # -- reference-mode IBM methods (lbm/lbm3d.py:66-167) -------------------------
     def flow_to_lagrange(self, *args, **kwargs):

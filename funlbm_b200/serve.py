@@ -1,0 +1,333 @@
+"""Serving: many independent simulations advanced together on one GPU.
+
+``LBMServer`` takes a stream of solve requests -- each one a funlbm config
+(any grid size, velocity set, storage, particles, faces) plus a step count
+and an arrival time -- and runs them with continuous batching:
+
+* **admission** -- a request is admitted as soon as it has arrived, a slot is
+  free and its estimated device memory fits in the HBM budget; requests that
+  arrive while others run join at the next chunk boundary, and finished ones
+  free their slot and memory at once;
+* **resident state** -- each admitted request keeps its populations,
+  particle state and IBM buffers on the device until it finishes;
+* **one launch per class per step** -- the fused step kernels of every
+  active lattice of the same (velocity set, storage, nodes per thread) run
+  in one multi-lattice launch (``lbm_flow_step_batch``); the particle
+  kernels of each lattice are issued around it in the reference's order;
+* **captured CUDA graphs** -- while the active set is unchanged, two steps of
+  the whole active set are captured once and replayed, so a step costs one
+  graph launch instead of dozens of kernel launches from Python.
+
+Each request's result (final rho, u and particle state) is the same as when
+it runs alone through ``LBMD3.run_step``: the batched kernel runs the same
+per-node code, and every launch shape gives the same bits.
+"""
+from __future__ import annotations
+
+import ctypes
+import itertools
+import time
+from dataclasses import dataclass, field
+from typing import Any, Dict, List, Optional
+
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+from .lattice import BYTES, ctypes_ref
+
+_ids = itertools.count()
+
+
+@dataclass
+class Request:
+    """One solve: a funlbm config dict, a step count and an arrival time (s)."""
+
+    config: Dict[str, Any]
+    steps: int
+    arrival: float = 0.0
+    rid: int = field(default_factory=lambda: next(_ids))
+    admitted_at: Optional[float] = None
+    finished_at: Optional[float] = None
+    result: Optional[Dict[str, Any]] = None
+    nodes: int = 0
+
+    @property
+    def latency(self):
+        return None if self.finished_at is None else self.finished_at - self.arrival
+
+
+def _shape_of(cfg):
+    size = (cfg.get("flow") or {}).get("size") or [100, 100, 100]
+    return tuple(int(s) + 1 for s in size)
+
+
+def estimate_bytes(cfg):
+    """Device memory one request holds while admitted: population buffers,
+    the reference-form tensors kept for observation, moments / force fields
+    and, with particles, the IBM buffers."""
+    flow = cfg.get("flow") or {}
+    q = int(str(flow.get("param_type") or "D3Q19")[3:])
+    storage = ((flow.get("precision") or {}).get("storage")) or flow.get("storage") or "fp32"
+    X, Y, Z = _shape_of(cfg)
+    n = X * Y * Z
+    pops = 2 * q * n * BYTES[storage] + 2 * 4 * q * n      # A/B + f and feq (float32)
+    fields = (3 + 1 + 1 + 3) * 4 * n                         # u, rho, p, FOL
+    ibm = (2 * 12 + 4) * n + 2 * (n // 32 + 1) if cfg.get("particles") else 0
+    return int(pops + fields + ibm + (8 << 20))
+
+
+class _Slot:
+    def __init__(self, req, lbm, nbytes):
+        self.req = req
+        self.lbm = lbm
+        self.nbytes = nbytes
+        self.remaining = req.steps
+        self.started = False
+
+
+class LBMServer:
+    """Continuous-batching server of LBM solves on one GPU."""
+
+    def __init__(self, budget_bytes=160e9, max_slots=256, device="cuda", use_graphs=True,
+                 chunk=32):
+        self.budget = int(budget_bytes)
+        self.max_slots = int(max_slots)
+        self.device = torch.device(device)
+        self.use_graphs = use_graphs
+        self.chunk = max(2, int(chunk))
+        self.queue: List[Request] = []
+        self.active: List[_Slot] = []
+        self.done: List[Request] = []
+        self.used = 0
+        self._graph = None
+        self._graph_key = None
+        self._graph_keep = None
+        self.stats = {"graph_captures": 0, "graph_replays": 0, "eager_steps": 0,
+                      "batched_launches": 0, "max_active": 0, "max_used_bytes": 0}
+
+    # -- queue ---------------------------------------------------------------
+    def submit(self, req: Request):
+        if estimate_bytes(req.config) > self.budget:
+            raise ValueError("request %d needs more device memory than the whole budget" % req.rid)
+        self.queue.append(req)
+        self.queue.sort(key=lambda r: r.arrival)
+
+    def _admit(self, now):
+        from .lbm import LBMD3, Config
+
+        admitted = False
+        i = 0
+        while i < len(self.queue) and len(self.active) < self.max_slots:
+            req = self.queue[i]
+            if req.arrival > now:
+                break
+            nbytes = estimate_bytes(req.config)
+            if self.used + nbytes > self.budget:
+                i += 1                      # first fit: a smaller request may go ahead
+                continue
+            self.queue.pop(i)
+            cfg = dict(req.config)
+            cfg.setdefault("log_per_steps", 10 ** 9)
+            cfg.setdefault("file", {"per_steps": 10 ** 9})
+            cfg["device"] = str(self.device)
+            lbm = LBMD3(config=Config().from_json(cfg))
+            lbm.init()
+            req.admitted_at = now
+            req.nodes = lbm.flow.n
+            self.active.append(_Slot(req, lbm, nbytes))
+            self.used += nbytes
+            admitted = True
+        self.stats["max_active"] = max(self.stats["max_active"], len(self.active))
+        self.stats["max_used_bytes"] = max(self.stats["max_used_bytes"], self.used)
+        return admitted
+
+    # -- one step of every active lattice --------------------------------------
+    @staticmethod
+    def _nodes_per_thread(lat):
+        return 2 if lat.shape[2] % 2 == 0 and lat.shape[2] >= 4 else 1
+
+    def _pack_tables(self, plans):
+        """Group the active lattices by (q, storage, nodes), pack their entries
+        into pinned host buffers and copy them to the device (stream-ordered).
+        Returns one launch description per group."""
+        groups = {}
+        for slot, plan in zip(self.active, plans):
+            lat = slot.lbm.flow.lattice
+            key = (lat.q, lat.storage, self._nodes_per_thread(lat))
+            groups.setdefault(key, []).append((slot, plan))
+        esize = _lib.load().lbm_batch_entry_bytes()
+        launches = []
+        for (q, storage, nodes), members in groups.items():
+            host = torch.empty(len(members) * esize, dtype=torch.uint8, pin_memory=True)
+            begin = torch.empty(len(members), dtype=torch.int32, pin_memory=True)
+            total = 0
+            force_any = False
+            for j, (slot, plan) in enumerate(members):
+                lat = slot.lbm.flow.lattice
+                nb = ctypes.c_uint32(0)
+                f = plan["force"]
+                call("lbm_batch_pack", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]),
+                     ptr(lat.buf[lat.cur ^ 1]), None if f is None else ctypes_ref(f),
+                     ptr(lat.face_rho[lat.cur]), ptr(lat.face_rho[lat.cur ^ 1]), ptr(lat.status),
+                     nodes, ctypes.c_void_p(host.data_ptr() + j * esize), ctypes.byref(nb))
+                begin[j] = total
+                total += nb.value
+                force_any = force_any or f is not None
+            dev = host.to(self.device, non_blocking=True)
+            dbegin = begin.to(self.device, non_blocking=True)
+            launches.append({"q": q, "storage": _lib.STORAGE[storage], "nodes": nodes,
+                             "force": int(force_any), "entries": dev, "begin": dbegin,
+                             "count": len(members), "blocks": total, "host": (host, begin),
+                             "forces": [p["force"] for _, p in members]})
+        return launches
+
+    def _step_all(self, launches=None, plans=None):
+        """Issue one fused step of every active lattice on the current stream:
+        the particle kernels of each lattice, one multi-lattice step launch per
+        group, the marker updates.  `launches` are prepared entry tables
+        (already on the device); without them the tables are packed now."""
+        s = _lib.stream_of(torch, self.device)
+        if plans is None:
+            plans = [slot.lbm.fused_prepare() for slot in self.active]
+        if launches is None:
+            launches = self._pack_tables(plans)
+        for L in launches:
+            call("lbm_flow_step_batch", L["q"], L["storage"], L["nodes"], L["force"],
+                 ptr(L["entries"]), ptr(L["begin"]), L["count"], L["blocks"], s)
+            self.stats["batched_launches"] += 1
+        for slot, plan in zip(self.active, plans):
+            fl = slot.lbm.flow
+            fl.stepped_elsewhere(plan["force"], plan["new_field"], plan["g_new"], keep=plan["keep"])
+            slot.lbm.fused_finish(plan)
+        return launches
+
+    def _eager_step(self):
+        self._step_all()
+        for slot in self.active:
+            slot.lbm.step += 1
+            slot.remaining -= 1
+            slot.started = True
+        self.stats["eager_steps"] += 1
+
+    def _graph_key_now(self):
+        return tuple((slot.req.rid, slot.lbm.flow.lattice.cur, getattr(slot.lbm, "_fi", 0),
+                      slot.lbm.step > 100) for slot in self.active)
+
+    def _flip(self, plans):
+        """Advance the buffer bookkeeping by one step without running it."""
+        for slot, plan in zip(self.active, plans):
+            slot.lbm.flow.lattice.cur ^= 1
+            if plan["ibm"]:
+                slot.lbm._fi ^= 1
+
+    def _graph_pair(self):
+        """Capture (once per active set) two steps of all active lattices and
+        run them.  Returns the graph, or None when it was just captured (the
+        capture run already advanced every lattice by two steps)."""
+        key = self._graph_key_now()
+        if self._graph is not None and key == self._graph_key:
+            return self._graph
+        self._graph = None
+        # entry tables of both steps, packed and uploaded before the capture
+        tables = []
+        for _ in range(2):
+            plans = [slot.lbm.fused_prepare(launch=False) for slot in self.active]
+            tables.append(self._pack_tables(plans))
+            self._flip(plans)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for t in tables:
+                self._step_all(launches=t)
+        g.replay()
+        self._graph = g
+        self._graph_keep = tables
+        self._graph_key = self._graph_key_now()
+        self.stats["graph_captures"] += 1
+        for slot in self.active:
+            slot.lbm.step += 2
+            slot.remaining -= 2
+        return None
+
+    def _advance(self, k):
+        """Advance every active lattice by k steps."""
+        done = 0
+        while done < k:
+            first = [slot for slot in self.active if not slot.started]
+            if first or not self.use_graphs or k - done < 2:
+                self._eager_step()
+                done += 1
+                continue
+            g = self._graph_pair()
+            if g is None:               # just captured: that ran two steps
+                done += 2
+                continue
+            g.replay()
+            self.stats["graph_replays"] += 1
+            for slot in self.active:
+                slot.lbm.step += 2
+                slot.remaining -= 2
+            done += 2
+
+    def _retire(self, now_fn):
+        keep = []
+        finished = []
+        for slot in self.active:
+            if slot.remaining <= 0:
+                finished.append(slot)
+            else:
+                keep.append(slot)
+        if not finished:
+            return False
+        for slot in finished:
+            lbm = slot.lbm
+            res = {"rho": lbm.flow.rou.clone(), "u": lbm.flow.u.clone(),
+                   "status": lbm.check_status(), "steps": lbm.step - 1}
+            ps = lbm.particle_swarm.particles
+            if ps:
+                res["cx"] = torch.stack([p.cx for p in ps]).clone()
+                res["cu"] = torch.stack([p.cu for p in ps]).clone()
+                res["cw"] = torch.stack([p.cw for p in ps]).clone()
+            slot.req.result = res
+        torch.cuda.synchronize(self.device)
+        t = now_fn()
+        for slot in finished:
+            slot.req.finished_at = t
+            self.used -= slot.nbytes
+            self.done.append(slot.req)
+            slot.lbm = None
+        self.active = keep
+        self._graph = None
+        return True
+
+    # -- main loop -------------------------------------------------------------
+    def run(self, requests=(), realtime=True):
+        """Serve `requests` (plus anything submitted before) to completion.
+        With realtime=True arrival times are honoured against the wall clock;
+        otherwise every request counts as arrived at t = 0."""
+        for r in requests:
+            self.submit(r)
+        t0 = time.perf_counter()
+
+        def now():
+            return time.perf_counter() - t0 if realtime else float("inf")
+
+        while self.queue or self.active:
+            changed = self._admit(now())
+            if changed:
+                self._graph = None
+            if not self.active:
+                if self.queue:
+                    wait = self.queue[0].arrival - now()
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
+                continue
+            k = min(self.chunk, min(slot.remaining for slot in self.active))
+            self._advance(k)
+            self._retire(lambda: time.perf_counter() - t0)
+        return self.done
+
+
+def storage_code(storage):
+    return _lib.STORAGE[storage]

@@ -132,6 +132,29 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
                   const float *face_rho_in, float *face_rho_out, const lbm_observe *obs,
                   uint32_t *status, void *stream);
 
+/* ---- many lattices per launch (serving) ---------------------------------
+ * One fused step (as lbm_flow_step) for up to thousands of independent
+ * lattices of one velocity set and storage in a single launch -- the form
+ * LBMBase.run_step (lbm/base.py:146-157) takes when many simulations are
+ * served together.  The caller packs one entry per lattice on the host
+ * (lbm_batch_pack, lbm_batch_entry_bytes() bytes each; the entry records the
+ * buffer addresses, so it is valid while they are), copies the entries and
+ * the exclusive prefix sum of their block counts to device memory, and
+ * launches.  A lattice's result is the same in a batch as alone. */
+size_t lbm_batch_entry_bytes(void);
+/* nodes: 1 (one node per thread) or 2 (two z-nodes per thread; rows of an
+ * even number >= 4 of nodes).  *blocks receives the lattice's block count. */
+int lbm_batch_pack(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
+                   const float *face_rho_in, float *face_rho_out, uint32_t *status, int32_t nodes,
+                   void *entry, uint32_t *blocks);
+/* entries / block_begin: device arrays of `count` packed entries (all with
+ * the same q, storage and nodes) and their first-block indices;
+ * total_blocks = sum of the block counts; force != 0 if any entry has a
+ * force. */
+int lbm_flow_step_batch(int32_t q, int32_t storage, int32_t nodes, int32_t force,
+                        const void *entries, const uint32_t *block_begin, int32_t count,
+                        uint32_t total_blocks, void *stream);
+
 /* Single reference functions on float32 SoA populations, for callers that
  * invoke FlowD3's methods one at a time. */
 /* FlowD3.cul_equ (flow/d3/base.py:150-159): f <- f - (f - feq)/tau in place;
