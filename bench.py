@@ -53,6 +53,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-size", type=int, default=64)
+    ap.add_argument("--serve", action="store_true",
+                    help="run the served-stream benchmark and print its own line")
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=[100, 600])
+    ap.add_argument("--serve-budget", type=float, default=160e9)
+    ap.add_argument("--serve-mode", default="streams", choices=["streams", "batched"])
+    ap.add_argument("--serve-particles", type=int, default=1,
+                    help="0: particle-free stream (for comparison)")
     ap.add_argument("--shape", default=None,
                     help="fixed launch shape 'nodes,threads' (e.g. 2,128 or -1,256) instead of "
                          "the autotuner")
@@ -322,6 +330,115 @@ def cpu_baseline(args, seconds=12.0):
                       % (n, steps, el, cores)}
 
 
+# ---------------------------------------------------------------------------
+# served stream (continuous batching) vs the same requests one by one
+# ---------------------------------------------------------------------------
+def make_requests(n, seed=0, steps=(500, 5000)):
+    """Seeded mixed stream: node counts per axis uniform in {32, 48, ..., 192},
+    D3Q19 / D3Q27 50/50, fp32 / fp16s 50/50, random WALL / PERIODICAL faces,
+    0-8 spheres or ellipsoids of radius 4-8, steps uniform in `steps`."""
+    from funlbm_b200.serve import Request
+
+    rng = np.random.default_rng(seed)
+    sizes = np.arange(32, 193, 16)
+    faces = ("input", "output", "back", "forward", "bottom", "top")
+    out = []
+    for _ in range(n):
+        dims = [int(v) for v in rng.choice(sizes, 3)]
+        q = 19 if rng.random() < 0.5 else 27
+        storage = "fp32" if rng.random() < 0.5 else "fp16s"
+        parts = []
+        for _ in range(int(rng.integers(0, 9))):
+            r = int(rng.integers(4, 9))
+            lo, hi = r + 3, [d - r - 4 for d in dims]
+            if min(hi) <= lo:
+                continue
+            center = [float(rng.uniform(lo, h)) for h in hi]
+            if rng.random() < 0.5:
+                parts.append({"type": "sphere", "r": r, "rou": 1.2, "coord": {"center": center}})
+            else:
+                rot = rng.uniform(-np.pi, np.pi, 3)
+                parts.append({"a": r, "b": max(2, round(0.75 * r)), "c": max(2, round(0.75 * r)),
+                              "rou": 1.2, "coord": {"center": center, "alpha": float(rot[0]),
+                                                    "beta": float(rot[1]), "gamma": float(rot[2])}})
+        cfg = {"device": "cuda", "log_per_steps": 10 ** 9, "file": {"per_steps": 10 ** 9},
+               "flow": {"size": [d - 1 for d in dims], "param_type": "D3Q%d" % q,
+                        "param": {"mu": 0.05, "gl": 1e-5}, "precision": {"storage": storage},
+                        "boundary": {k: {"code": str(rng.choice(["WALL", "PERIODICAL"]))}
+                                     for k in faces}},
+               "particles": parts}
+        out.append(Request(cfg, int(rng.integers(steps[0], steps[1] + 1))))
+    return out
+
+
+def run_serve(args):
+    """Served stream vs one-by-one: aggregate MLUPS with every request queued
+    at t = 0, p50/p99 time-to-result with Poisson arrivals at 80 % of that
+    capacity, and the same requests sequentially through LBMD3.run_step."""
+    import copy
+
+    import torch
+
+    from funlbm_b200.lbm import LBMD3, Config
+    from funlbm_b200.serve import LBMServer, Request
+
+    base = make_requests(args.serve_requests, seed=5, steps=tuple(args.serve_steps))
+    if not args.serve_particles:
+        for r in base:
+            r.config["particles"] = []
+    work = sum(r.steps * np.prod([d + 1 for d in r.config["flow"]["size"]]) for r in base)
+
+    # sequential: each request alone through the plain path
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in base:
+        lbm = LBMD3(config=Config().from_json(copy.deepcopy(r.config)))
+        lbm.init()
+        for _ in range(r.steps):
+            lbm.run_step(step=lbm.step)
+            lbm.step += 1
+        lbm.flow.rou.sum().item()
+        del lbm
+    seq_s = time.perf_counter() - t0
+    torch.cuda.empty_cache()
+
+    # served, saturated (everything queued at t = 0)
+    server = LBMServer(budget_bytes=args.serve_budget, chunk=32, mode=args.serve_mode)
+    reqs = [Request(copy.deepcopy(r.config), r.steps) for r in base]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    server.run(reqs, realtime=False)
+    sat_s = time.perf_counter() - t0
+    stats_sat = dict(server.stats)
+    del server
+    torch.cuda.empty_cache()
+
+    # served, Poisson arrivals at 80 % of the saturated capacity
+    rate = 0.8 * len(base) / sat_s
+    rng = np.random.default_rng(11)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(base)))
+    server = LBMServer(budget_bytes=args.serve_budget, chunk=32, mode=args.serve_mode)
+    reqs = [Request(copy.deepcopy(r.config), r.steps, arrival=float(a))
+            for r, a in zip(base, arrivals)]
+    t0 = time.perf_counter()
+    server.run(reqs, realtime=True)
+    poi_s = time.perf_counter() - t0
+    lat = np.array([r.latency for r in reqs])
+    return {
+        "requests": len(base), "lattice_updates": float(work),
+        "steps_range": list(args.serve_steps),
+        "served_mlups": work / sat_s / 1e6, "sequential_mlups": work / seq_s / 1e6,
+        "speedup_vs_sequential": seq_s / sat_s,
+        "served_s": sat_s, "sequential_s": seq_s,
+        "poisson": {"rate_per_s": rate, "makespan_s": poi_s, "p50_s": float(np.percentile(lat, 50)),
+                    "p99_s": float(np.percentile(lat, 99)),
+                    "aggregate_mlups": work / poi_s / 1e6},
+        "budget_gb": args.serve_budget / 1e9, "mode": args.serve_mode,
+        "stats_saturated": stats_sat,
+        "note": "sequential = each request alone through LBMD3.run_step (plain fused path)",
+    }
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -387,6 +504,13 @@ def main():
 
     build.build()
     world, rank, local = dist_setup(args)
+    if args.serve:
+        if rank == 0:
+            res = run_serve(args)
+            print(json.dumps({"metric": "served stream: aggregate MLUPS and p50/p99 time-to-result "
+                                        "vs the same requests one by one", "value": res["served_mlups"],
+                              "unit": "MLUPS", "higher_is_better": True, "serve": res}), flush=True)
+        return 0
     n = args.size
     ms, clocks, status, launch = run_device(args, world, rank, local)
     ms_per_step = ms / args.steps

@@ -395,9 +395,9 @@ int lbm_batch_pack(const lbm_lattice *lat, const void *fa, void *fb, const lbm_f
               "(>= 4) of nodes");
     return LBM_ERR_INVALID;
   }
-  const long long threads = nodes == 2 ? 128 : 256;
+  const long long per_block = (nodes == 2 ? 128 : 256) * (long long)kBatchTiles;
   const long long work = a.g.n / nodes;
-  *blocks = (uint32_t)((work + threads - 1) / threads);
+  *blocks = (uint32_t)((work + per_block - 1) / per_block);
   memcpy(entry, &a, sizeof(a));
   return LBM_OK;
 }

@@ -238,9 +238,11 @@ __global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
 // [block_begin[e], block_begin[e+1]); each block finds its lattice by binary
 // search, copies that lattice's StepArgs into shared memory and runs the
 // same per-node code as the single-lattice kernels (NZ = 1: k_step's body,
-// NZ > 1: k_step_vec's), so a lattice's result does not depend on which
-// other lattices share the launch.
+// NZ > 1: k_step_vec's) on kBatchTiles consecutive tiles, so a lattice's
+// result does not depend on which other lattices share the launch.
 // ---------------------------------------------------------------------------
+constexpr int kBatchTiles = 4;   // tiles of TB threads per block (amortises the lookup)
+
 template <int Q, int S, bool FORCE, int NZ, int TB>
 __global__ void __launch_bounds__(TB)
     k_step_batch(const StepArgs *__restrict__ entries, const unsigned *__restrict__ block_begin,
@@ -266,11 +268,14 @@ __global__ void __launch_bounds__(TB)
   unsigned *dst = reinterpret_cast<unsigned *>(&sa);
   for (int w = threadIdx.x; w < kWordsArgs; w += TB) dst[w] = src[w];
   __syncthreads();
-  const unsigned t = (blockIdx.x - block_begin[e]) * TB + threadIdx.x;
-  if constexpr (NZ == 1)
-    step_scalar_body<Q, S, FORCE>(sa, t);
-  else
-    step_vec_body<Q, S, FORCE, NZ>(sa, t);
+  const unsigned t0 = (blockIdx.x - block_begin[e]) * (TB * kBatchTiles) + threadIdx.x;
+#pragma unroll 1
+  for (int it = 0; it < kBatchTiles; ++it) {
+    if constexpr (NZ == 1)
+      step_scalar_body<Q, S, FORCE>(sa, t0 + it * TB);
+    else
+      step_vec_body<Q, S, FORCE, NZ>(sa, t0 + it * TB);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -315,10 +315,18 @@ class Particle:
             self.coord.angle = torch.tensor(np.asarray(group.get("angle")[:]))
 
 
+_MARKER_CACHE = {}
+
+
 def _markers_tensor(ra, rb, rc, dx, device):
-    pts = generate_uniform_points_on_ellipsoid(-ra - 2 * dx, -rb - 2 * dx, -rc - 2 * dx,
-                                               ra + 2 * dx, rb + 2 * dx, rc + 2 * dx,
-                                               dx=dx, semi_axes=(ra, rb, rc))
+    """Body-frame markers of an ellipsoid (a sphere when ra = rb = rc); the
+    generator is deterministic, so each shape is computed once per process."""
+    key = (float(ra), float(rb), float(rc), float(dx))
+    if key not in _MARKER_CACHE:
+        _MARKER_CACHE[key] = generate_uniform_points_on_ellipsoid(
+            -ra - 2 * dx, -rb - 2 * dx, -rc - 2 * dx, ra + 2 * dx, rb + 2 * dx, rc + 2 * dx,
+            dx=dx, semi_axes=(ra, rb, rc))
+    pts = _MARKER_CACHE[key]
     return torch.tensor(pts, device=device, dtype=torch.float32).reshape(-1, 3)
 
 

@@ -84,13 +84,34 @@ class _Slot:
         self.nbytes = nbytes
         self.remaining = req.steps
         self.started = False
+        self.stream = None
+        self.graphs = []
+        self.done = None
 
 
 class LBMServer:
-    """Continuous-batching server of LBM solves on one GPU."""
+    """Continuous-batching server of LBM solves on one GPU.
+
+    mode="streams" (default): every admitted request gets a stream from a
+    pool and its own CUDA graphs of up to `graph_steps` steps (captured
+    without a device synchronisation); its whole run is enqueued at
+    admission and overlaps on the device with the others.  Completion is polled with events, so
+    finishing or admitting a request never stalls the rest.
+
+    mode="batched": all active lattices of one (velocity set, storage, nodes
+    per thread) advance together in one multi-lattice step launch per step;
+    two steps of the whole active set are captured as one graph, recaptured
+    whenever the active set changes.
+    """
 
     def __init__(self, budget_bytes=160e9, max_slots=256, device="cuda", use_graphs=True,
-                 chunk=32):
+                 chunk=32, mode="streams", streams=32, graph_steps=64):
+        if mode not in ("streams", "batched"):
+            raise ValueError("mode must be 'streams' or 'batched'")
+        self.mode = mode
+        self.graph_steps = max(2, int(graph_steps) - int(graph_steps) % 2)
+        self._streams = [torch.cuda.Stream(device=device) for _ in range(max(1, int(streams)))]
+        self._next_stream = 0
         self.budget = int(budget_bytes)
         self.max_slots = int(max_slots)
         self.device = torch.device(device)
@@ -104,7 +125,8 @@ class LBMServer:
         self._graph_key = None
         self._graph_keep = None
         self.stats = {"graph_captures": 0, "graph_replays": 0, "eager_steps": 0,
-                      "batched_launches": 0, "max_active": 0, "max_used_bytes": 0}
+                      "batched_launches": 0, "max_active": 0, "max_used_bytes": 0,
+                      "t_admit": 0.0, "t_capture": 0.0, "t_steps": 0.0, "t_retire": 0.0}
 
     # -- queue ---------------------------------------------------------------
     def submit(self, req: Request):
@@ -131,21 +153,113 @@ class LBMServer:
             cfg.setdefault("log_per_steps", 10 ** 9)
             cfg.setdefault("file", {"per_steps": 10 ** 9})
             cfg["device"] = str(self.device)
-            lbm = LBMD3(config=Config().from_json(cfg))
-            lbm.init()
+            if self.mode == "streams":
+                stream = self._streams[self._next_stream % len(self._streams)]
+                self._next_stream += 1
+                with torch.cuda.stream(stream):
+                    lbm = LBMD3(config=Config().from_json(cfg))
+                    lbm.init()
+                    slot = _Slot(req, lbm, nbytes)
+                    slot.stream = stream
+                    self._enqueue_run(slot)
+            else:
+                lbm = LBMD3(config=Config().from_json(cfg))
+                lbm.init()
+                slot = _Slot(req, lbm, nbytes)
             req.admitted_at = now
             req.nodes = lbm.flow.n
-            self.active.append(_Slot(req, lbm, nbytes))
+            self.active.append(slot)
             self.used += nbytes
             admitted = True
         self.stats["max_active"] = max(self.stats["max_active"], len(self.active))
         self.stats["max_used_bytes"] = max(self.stats["max_used_bytes"], self.used)
         return admitted
 
+    # -- streams mode --------------------------------------------------------------
+    def _capture_steps(self, lbm, stream, n):
+        """Capture n (even) fused steps of one lattice on `stream` (no device
+        sync; nothing runs).  The bookkeeping returns to the same buffers after
+        an even number of steps, so the graph can be replayed any number of
+        times."""
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            g.capture_begin()
+            try:
+                for _ in range(n):
+                    lbm._fused_step()
+            finally:
+                g.capture_end()
+        self.stats["graph_captures"] += 1
+        return g
+
+    def _enqueue_run(self, slot):
+        """Enqueue the whole run of one request on its stream: the first step
+        eagerly (it enters the fused representation and allocates), then
+        replays of captured graphs of up to `graph_steps` steps -- separate
+        graphs for steps up to 100 and after, because the interpolation's
+        weight-sum check (active after step 100, lbm/lbm3d.py:84) is a
+        parameter of the captured launches -- and eager steps for what is
+        left over."""
+        lbm, rem = slot.lbm, slot.remaining
+        s = slot.stream
+        with torch.cuda.stream(s):
+            lbm.run_step(step=lbm.step)
+            lbm.step += 1
+            rem -= 1
+            self.stats["eager_steps"] += 1
+            while rem > 0:
+                if self.use_graphs and rem >= 2:
+                    span = rem if lbm.step > 100 else min(rem, 101 - lbm.step)
+                    n = min(self.graph_steps, span)
+                    n -= n % 2
+                    if n >= 2:
+                        reps = span // n
+                        g = self._capture_steps(lbm, s, n)
+                        slot.graphs.append(g)
+                        for _ in range(reps):
+                            g.replay()
+                        self.stats["graph_replays"] += reps
+                        lbm.step += n * reps
+                        rem -= n * reps
+                        continue
+                lbm.run_step(step=lbm.step)
+                lbm.step += 1
+                rem -= 1
+                self.stats["eager_steps"] += 1
+            slot.done = torch.cuda.Event()
+            slot.done.record(s)
+        slot.remaining = 0
+
+    def _retire_streams(self, now_fn):
+        finished = [slot for slot in self.active if slot.done is not None and slot.done.query()]
+        if not finished:
+            return False
+        for slot in finished:
+            lbm = slot.lbm
+            with torch.cuda.stream(slot.stream):
+                res = {"rho": lbm.flow.rou.clone(), "u": lbm.flow.u.clone(),
+                       "status": lbm.check_status(), "steps": lbm.step - 1}
+                ps = lbm.particle_swarm.particles
+                if ps:
+                    res["cx"] = torch.stack([p.cx for p in ps]).clone()
+                    res["cu"] = torch.stack([p.cu for p in ps]).clone()
+                    res["cw"] = torch.stack([p.cw for p in ps]).clone()
+            slot.stream.synchronize()
+            slot.req.result = res
+            slot.req.finished_at = now_fn()
+            self.used -= slot.nbytes
+            self.done.append(slot.req)
+            slot.graphs = []
+            slot.lbm = None
+        self.active = [slot for slot in self.active if slot not in finished]
+        return True
+
     # -- one step of every active lattice --------------------------------------
     @staticmethod
     def _nodes_per_thread(lat):
-        return 2 if lat.shape[2] % 2 == 0 and lat.shape[2] >= 4 else 1
+        # two z-nodes per thread for float32 rows of even length; 16-bit
+        # storage runs fastest with one node per thread
+        return 2 if lat.storage == "fp32" and lat.shape[2] % 2 == 0 and lat.shape[2] >= 4 else 1
 
     def _pack_tables(self, plans):
         """Group the active lattices by (q, storage, nodes), pack their entries
@@ -187,19 +301,45 @@ class LBMServer:
         the particle kernels of each lattice, one multi-lattice step launch per
         group, the marker updates.  `launches` are prepared entry tables
         (already on the device); without them the tables are packed now."""
+        main = torch.cuda.current_stream(self.device)
         s = _lib.stream_of(torch, self.device)
+        ibm = [slot for slot in self.active if slot.lbm.particle_swarm.particles]
+        side = {}
+        pool = self._streams[1:] or self._streams   # streams[0] captures the batched graph
+        for j, slot in enumerate(ibm):            # fork: one branch per particle lattice
+            sj = pool[j % len(pool)]
+            sj.wait_stream(main)
+            side[id(slot)] = sj
         if plans is None:
-            plans = [slot.lbm.fused_prepare() for slot in self.active]
+            plans = []
+            for slot in self.active:
+                sj = side.get(id(slot))
+                if sj is None:
+                    plans.append(slot.lbm.fused_prepare())
+                else:
+                    with torch.cuda.stream(sj):
+                        plans.append(slot.lbm.fused_prepare())
+        for sj in set(side.values()):             # join before the step launches
+            main.wait_stream(sj)
         if launches is None:
             launches = self._pack_tables(plans)
         for L in launches:
             call("lbm_flow_step_batch", L["q"], L["storage"], L["nodes"], L["force"],
                  ptr(L["entries"]), ptr(L["begin"]), L["count"], L["blocks"], s)
             self.stats["batched_launches"] += 1
+        for sj in set(side.values()):
+            sj.wait_stream(main)
         for slot, plan in zip(self.active, plans):
             fl = slot.lbm.flow
             fl.stepped_elsewhere(plan["force"], plan["new_field"], plan["g_new"], keep=plan["keep"])
-            slot.lbm.fused_finish(plan)
+            sj = side.get(id(slot))
+            if sj is None:
+                slot.lbm.fused_finish(plan)
+            else:
+                with torch.cuda.stream(sj):
+                    slot.lbm.fused_finish(plan)
+        for sj in set(side.values()):             # join the marker updates
+            main.wait_stream(sj)
         return launches
 
     def _eager_step(self):
@@ -229,22 +369,30 @@ class LBMServer:
         if self._graph is not None and key == self._graph_key:
             return self._graph
         self._graph = None
+        tc = time.perf_counter()
         # entry tables of both steps, packed and uploaded before the capture
         tables = []
         for _ in range(2):
             plans = [slot.lbm.fused_prepare(launch=False) for slot in self.active]
             tables.append(self._pack_tables(plans))
             self._flip(plans)
-        torch.cuda.synchronize(self.device)
+        cap = self._streams[0]
+        cap.wait_stream(torch.cuda.current_stream(self.device))
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            for t in tables:
-                self._step_all(launches=t)
+        with torch.cuda.stream(cap):
+            g.capture_begin()
+            try:
+                for t in tables:
+                    self._step_all(launches=t)
+            finally:
+                g.capture_end()
+        torch.cuda.current_stream(self.device).wait_stream(cap)
         g.replay()
         self._graph = g
         self._graph_keep = tables
         self._graph_key = self._graph_key_now()
         self.stats["graph_captures"] += 1
+        self.stats["t_capture"] += time.perf_counter() - tc
         for slot in self.active:
             slot.lbm.step += 2
             slot.remaining -= 2
@@ -313,8 +461,26 @@ class LBMServer:
         def now():
             return time.perf_counter() - t0 if realtime else float("inf")
 
+        if self.mode == "streams":
+            while self.queue or self.active:
+                ta = time.perf_counter()
+                self._admit(now())
+                self.stats["t_admit"] += time.perf_counter() - ta
+                tr = time.perf_counter()
+                retired = self._retire_streams(lambda: time.perf_counter() - t0)
+                self.stats["t_retire"] += time.perf_counter() - tr
+                if not retired:
+                    if self.queue and not self.active:
+                        wait = self.queue[0].arrival - now()
+                        time.sleep(min(max(wait, 0.0), 0.05))
+                    else:
+                        time.sleep(2e-4)
+            torch.cuda.synchronize(self.device)
+            return self.done
         while self.queue or self.active:
+            ta = time.perf_counter()
             changed = self._admit(now())
+            self.stats["t_admit"] += time.perf_counter() - ta
             if changed:
                 self._graph = None
             if not self.active:
@@ -324,8 +490,12 @@ class LBMServer:
                         time.sleep(min(wait, 0.05))
                 continue
             k = min(self.chunk, min(slot.remaining for slot in self.active))
+            ts = time.perf_counter()
             self._advance(k)
+            tr = time.perf_counter()
+            self.stats["t_steps"] += tr - ts
             self._retire(lambda: time.perf_counter() - t0)
+            self.stats["t_retire"] += time.perf_counter() - tr
         return self.done
 
 
