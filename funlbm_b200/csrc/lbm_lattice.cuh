@@ -115,10 +115,19 @@ struct Storage;
 
 // from_bits / to_bits convert one stored element held in the low bits of a
 // 32-bit word (used by the vectorised loads and stores).
+//
+// The fused step works on the stored quantity itself (its "working value"):
+// f for FP32, the deviation d = f - w_i for the shifted forms (kDev), whose
+// moments and collision are restated for d (dev_moments / collide_dev), so
+// no weight is added on load or subtracted on store.  work / put / work2 /
+// put2 move working values; load / store always give f.
 template <>
 struct Storage<LBM_STORAGE_FP32> {
   using T = float;
   static constexpr int kBits = 32;
+  static constexpr bool kDev = false;
+  __device__ __forceinline__ static float work(const T *p) { return __ldg(p); }
+  __device__ __forceinline__ static void put(T *p, float v) { *p = v; }
   __device__ __forceinline__ static float load(const T *p, float) { return __ldg(p); }
   __device__ __forceinline__ static void store(T *p, float v, float) { *p = v; }
   __device__ __forceinline__ static float from_bits(unsigned b, float) { return __uint_as_float(b); }
@@ -128,6 +137,9 @@ template <>
 struct Storage<LBM_STORAGE_FP16S> {
   using T = __half;
   static constexpr int kBits = 16;
+  static constexpr bool kDev = true;
+  __device__ __forceinline__ static float work(const T *p) { return __half2float(__ldg(p)); }
+  __device__ __forceinline__ static void put(T *p, float v) { *p = __float2half_rn(v); }
   __device__ __forceinline__ static float load(const T *p, float w) {
     return w + __half2float(__ldg(p));
   }
@@ -145,6 +157,9 @@ template <>
 struct Storage<LBM_STORAGE_BF16S> {
   using T = __nv_bfloat16;
   static constexpr int kBits = 16;
+  static constexpr bool kDev = true;
+  __device__ __forceinline__ static float work(const T *p) { return __bfloat162float(__ldg(p)); }
+  __device__ __forceinline__ static void put(T *p, float v) { *p = __float2bfloat16_rn(v); }
   __device__ __forceinline__ static float load(const T *p, float w) {
     return w + __bfloat162float(__ldg(p));
   }
@@ -185,6 +200,36 @@ __device__ __forceinline__ unsigned pack2<LBM_STORAGE_FP16S>(float a, float b, f
 template <>
 __device__ __forceinline__ unsigned pack2<LBM_STORAGE_BF16S>(float a, float b, float w) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a - w, b - w);
+  unsigned word;
+  memcpy(&word, &h, 4);
+  return word;
+}
+
+// Two consecutive stored elements <-> two working values (low element first).
+template <int S>
+__device__ __forceinline__ float2 work2(unsigned word);
+template <>
+__device__ __forceinline__ float2 work2<LBM_STORAGE_FP16S>(unsigned word) {
+  __half2 h;
+  memcpy(&h, &word, 4);
+  return __half22float2(h);
+}
+template <>
+__device__ __forceinline__ float2 work2<LBM_STORAGE_BF16S>(unsigned word) {
+  return make_float2(__uint_as_float(word << 16), __uint_as_float(word & 0xffff0000u));
+}
+template <int S>
+__device__ __forceinline__ unsigned put2(float a, float b);
+template <>
+__device__ __forceinline__ unsigned put2<LBM_STORAGE_FP16S>(float a, float b) {
+  const __half2 h = __floats2half2_rn(a, b);
+  unsigned word;
+  memcpy(&word, &h, 4);
+  return word;
+}
+template <>
+__device__ __forceinline__ unsigned put2<LBM_STORAGE_BF16S>(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
   unsigned word;
   memcpy(&word, &h, 4);
   return word;
@@ -263,22 +308,13 @@ __device__ __forceinline__ bool on_any_face(const Geom &g, int x, int y, int z) 
 //   WALL_WITH_SPEED face -> (t, rev(i)) - 2 rho_t w_i (e_i . uw) / cs^2
 // NON_EQUILIBRIUM x faces are handled by the caller (they need moments).
 // ---------------------------------------------------------------------------
-template <int Q, int S>
-__device__ __forceinline__ void pull_interior(const typename Storage<S>::T *__restrict__ fa,
-                                              const Geom &g, long long idx, float f[Q]) {
-  using V = VSet<Q>;
-  static_for<Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    const long long off = (long long)V::ex(i) * g.nyz + (long long)V::ey(i) * g.nz + V::ez(i);
-    f[i] = Storage<S>::load(fa + (long long)i * g.n + idx - off, V::w(i));
-  });
-}
-
 // Pull population I with face rules.  The governing face is the last one in
 // the order x, y, z whose plane holds the node and through which direction I
 // enters; -1 means none.  `face_rho` is consulted only for WALL_WITH_SPEED
 // faces (density of the previous step at this face node).
-template <int Q, int S, int I>
+// WORK: return the storage's working value (d for the shifted forms) instead
+// of f; the WALL_WITH_SPEED correction is the same in both.
+template <int Q, int S, int I, bool WORK = false>
 __device__ __forceinline__ float pull_one(const typename Storage<S>::T *__restrict__ fa,
                                           const Geom &g, int x, int y, int z,
                                           const float *__restrict__ face_rho) {
@@ -315,30 +351,33 @@ __device__ __forceinline__ float pull_one(const typename Storage<S>::T *__restri
   }
   const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;
   const float w_sd = sd == I ? V::w(I) : V::w(V::rev(I));
-  return Storage<S>::load(fa + (long long)sd * g.n + src, w_sd) - corr;
+  if constexpr (WORK)
+    return Storage<S>::work(fa + (long long)sd * g.n + src) - corr;
+  else
+    return Storage<S>::load(fa + (long long)sd * g.n + src, w_sd) - corr;
 }
 
-template <int Q, int S, int I = 0>
+template <int Q, int S, bool WORK, int I = 0>
 struct PullGeneral {
   __device__ __forceinline__ static void run(const typename Storage<S>::T *__restrict__ fa,
                                              const Geom &g, int x, int y, int z,
                                              const float *__restrict__ face_rho, float f[Q]) {
-    f[I] = pull_one<Q, S, I>(fa, g, x, y, z, face_rho);
-    PullGeneral<Q, S, I + 1>::run(fa, g, x, y, z, face_rho, f);
+    f[I] = pull_one<Q, S, I, WORK>(fa, g, x, y, z, face_rho);
+    PullGeneral<Q, S, WORK, I + 1>::run(fa, g, x, y, z, face_rho, f);
   }
 };
-template <int Q, int S>
-struct PullGeneral<Q, S, Q> {
+template <int Q, int S, bool WORK>
+struct PullGeneral<Q, S, WORK, Q> {
   __device__ __forceinline__ static void run(const typename Storage<S>::T *__restrict__,
                                              const Geom &, int, int, int,
                                              const float *__restrict__, float *) {}
 };
 
-template <int Q, int S>
+template <int Q, int S, bool WORK = false>
 __device__ __forceinline__ void pull_general(const typename Storage<S>::T *__restrict__ fa,
                                              const Geom &g, int x, int y, int z,
                                              const float *__restrict__ face_rho, float f[Q]) {
-  PullGeneral<Q, S>::run(fa, g, x, y, z, face_rho, f);
+  PullGeneral<Q, S, WORK>::run(fa, g, x, y, z, face_rho, f);
 }
 
 // Rolled value (periodic wrap on every axis, no face rule): what the
@@ -480,6 +519,69 @@ __device__ __forceinline__ void collide(float f[Q], const Geom &g, float rho, fl
       const float b = ow * t;
       f[i] = LBM_FMA(f[i], keep, a + b);
       f[j] = LBM_FMA(f[j], keep, a - b);
+    }
+  });
+}
+
+// Deviation form, for the shifted storages.  With f_i = w_i + d_i,
+// sum w_i = 1 and sum w_i e_i = 0:
+//   rho = 1 + sum d_i,   rho u = sum d_i e_i + F/2,
+// and the BGK update of FlowD3.cul_equ (flow/d3/base.py:150-159) becomes
+//   d_i <- d_i (1 - 1/tau) + (feq_i - w_i) / tau,
+//   feq_i - w_i = w_i [ (rho - 1) + rho (t + t^2/2 - |u|^2/(2 cs^2)) ],
+// so the pair (i, rev(i)) gets A +- B with
+//   A = w (drho - rho |u|^2/(2cs^2)) / tau + (w rho t / (2 tau)) t,  B = w rho t / tau.
+// The forcing term (add_force) is additive and applies to d unchanged.
+template <int Q>
+__device__ __forceinline__ void dev_moments(const float d[Q], float fx, float fy, float fz,
+                                            bool face, float &rho, float &drho, float &ux,
+                                            float &uy, float &uz) {
+  using V = VSet<Q>;
+  float r = d[0], jx = 0.f, jy = 0.f, jz = 0.f;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int j = V::rev(i);
+    if constexpr (i != 0 && i < j) {
+      const float s = d[i] + d[j];
+      const float t = d[i] - d[j];
+      r += s;
+      if constexpr (V::ex(i) > 0) jx += t;
+      if constexpr (V::ex(i) < 0) jx -= t;
+      if constexpr (V::ey(i) > 0) jy += t;
+      if constexpr (V::ey(i) < 0) jy -= t;
+      if constexpr (V::ez(i) > 0) jz += t;
+      if constexpr (V::ez(i) < 0) jz -= t;
+    }
+  });
+  drho = r;
+  rho = 1.f + r;
+  const float inv = __fdividef(1.f, rho);
+  ux = face ? 0.f : LBM_FMA(0.5f, fx, jx) * inv;
+  uy = face ? 0.f : LBM_FMA(0.5f, fy, jy) * inv;
+  uz = face ? 0.f : LBM_FMA(0.5f, fz, jz) * inv;
+}
+
+template <int Q>
+__device__ __forceinline__ void collide_dev(float d[Q], const Geom &g, float rho, float drho,
+                                            float ux, float uy, float uz) {
+  using V = VSet<Q>;
+  const float u2 = LBM_FMA(ux, ux, LBM_FMA(uy, uy, uz * uz)) * (0.5f * g.inv_cs2);
+  const float vx = ux * g.inv_cs2, vy = uy * g.inv_cs2, vz = uz * g.inv_cs2;
+  const float om = g.inv_tau, keep = 1.f - g.inv_tau;
+  const float orho = om * rho;
+  const float c = om * LBM_FMA(-rho, u2, drho);
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int j = V::rev(i);
+    constexpr float w = V::w(i);
+    if constexpr (i == 0) {
+      d[0] = LBM_FMA(d[0], keep, w * c);
+    } else if constexpr (i < j) {
+      const float t = edot<Q, i>(vx, vy, vz);
+      const float a = LBM_FMA((orho * (0.5f * w)) * t, t, w * c);
+      const float b = (orho * w) * t;
+      d[i] = LBM_FMA(d[i], keep, a + b);
+      d[j] = LBM_FMA(d[j], keep, a - b);
     }
   });
 }

@@ -11,10 +11,28 @@
 namespace lbm {
 
 constexpr int kThreads = 256;
+constexpr int kMaxQ = 27;
 
 // ---------------------------------------------------------------------------
 // Fused step
 // ---------------------------------------------------------------------------
+// Per-direction plane pointers of one step, computed on the host
+// (fill_step_planes), so that every population address in the kernels is
+// one 32 x 32 -> 64-bit multiply-add of the node index onto a parameter:
+//   src[i] + idx   row (x - ex, y - ey) of plane i of fa at the node's z: the
+//                  pull source of an interior row is src[i] + idx - ez;
+//   zlo[i] + idx   (ez > 0) source of a node at z = 0 under the bottom face
+//                  rule: PERIODICAL -> (i, x, y, nz - 1), else (rev i, x, y, 0);
+//   zhi[i] + idx   (ez < 0) source of a node at z = nz - 1 under the top face
+//                  rule: PERIODICAL -> (i, x, y, 0), else (rev i, x, y, nz - 1);
+//   dst[i] + idx   plane i of fb.
+struct StepPlanes {
+  const void *src[kMaxQ];
+  const void *zlo[kMaxQ];
+  const void *zhi[kMaxQ];
+  void *dst[kMaxQ];
+};
+
 struct StepArgs {
   Geom g;
   NodeDecomp dec;
@@ -27,6 +45,7 @@ struct StepArgs {
   float *face_rho_out;
   float *obs_f, *obs_rho, *obs_u;
   unsigned *status;
+  StepPlanes p;
 };
 
 template <int Q>
@@ -40,12 +59,22 @@ __device__ __forceinline__ void write_face_rho(const Geom &g, float *out, int x,
   if (z == g.nz - 1) out[plane_index(g, 5, x, y, z)] = rho;
 }
 
+__device__ __forceinline__ unsigned bad_bits(float rho, float ux, float uy, float uz) {
+  unsigned b = 0;
+  if (!(rho > 0.f) || !(rho < 3.0e38f)) b |= LBM_STATUS_RHO_BAD;
+  if (!(fabsf(ux) + fabsf(uy) + fabsf(uz) < 3.0e38f)) b |= LBM_STATUS_U_BAD;
+  return b;
+}
+
 // Everything after the pull for one node: the previous / new forcing, the
-// moment passes, cul_equ2, status, face densities, observation, and (when
-// fb is set) the next step's collision, in place in f.
-template <int Q, bool FORCE>
+// moment passes, cul_equ2, status bits (accumulated in `bad`), face
+// densities, observation, and (when fb is set) the next step's collision, in
+// place in f.  DEV: f holds deviations d = f - w (shifted storage), handled
+// by dev_moments / collide_dev.
+template <int Q, bool FORCE, bool DEV>
 __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsigned idx, int x,
-                                            int y, int z, bool face) {
+                                            int y, int z, bool face, unsigned &bad) {
+  using V = VSet<Q>;
   float fox = a.go[0], foy = a.go[1], foz = a.go[2];
   float fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
   if (a.fol_old != nullptr && (a.ch_old == nullptr || a.ch_old[idx >> 5])) {
@@ -58,18 +87,24 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsig
     fny += a.fol_new[3ull * idx + 1];
     fnz += a.fol_new[3ull * idx + 2];
   }
-  float rho, ux, uy, uz;
-  moments<Q>(f, fox, foy, foz, face, rho, ux, uy, uz);
+  float rho, drho = 0.f, ux, uy, uz;
+  if constexpr (DEV)
+    dev_moments<Q>(f, fox, foy, foz, face, rho, drho, ux, uy, uz);
+  else
+    moments<Q>(f, fox, foy, foz, face, rho, ux, uy, uz);
   if (FORCE) {
     add_force<Q>(f, a.g, ux, uy, uz, fnx, fny, fnz);
-    moments<Q>(f, fnx, fny, fnz, face, rho, ux, uy, uz);
+    if constexpr (DEV)
+      dev_moments<Q>(f, fnx, fny, fnz, face, rho, drho, ux, uy, uz);
+    else
+      moments<Q>(f, fnx, fny, fnz, face, rho, ux, uy, uz);
   }
-  flag_bad(a.status, rho, ux, uy, uz);
+  bad |= bad_bits(rho, ux, uy, uz);
   if (face && a.face_rho_out != nullptr) write_face_rho<Q>(a.g, a.face_rho_out, x, y, z, rho);
   if (a.obs_f != nullptr) {
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      a.obs_f[(long long)i * a.g.n + idx] = f[i];
+      a.obs_f[(long long)i * a.g.n + idx] = DEV ? f[i] + V::w(i) : f[i];
     });
   }
   if (a.obs_rho != nullptr) a.obs_rho[idx] = rho;
@@ -78,35 +113,90 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsig
     a.obs_u[3ull * idx + 1] = uy;
     a.obs_u[3ull * idx + 2] = uz;
   }
-  if (a.fb != nullptr) collide<Q>(f, a.g, rho, ux, uy, uz);
+  if (a.fb != nullptr) {
+    if constexpr (DEV)
+      collide_dev<Q>(f, a.g, rho, drho, ux, uy, uz);
+    else
+      collide<Q>(f, a.g, rho, ux, uy, uz);
+  }
+}
+
+__device__ __forceinline__ void report_bad(unsigned *status, unsigned bad) {
+  if (bad != 0 && status != nullptr) atomicOr(status, bad);
+}
+
+// WALL_WITH_SPEED correction of the directions entering through z face FC
+// (4 = bottom, 5 = top) at a node of an interior row, applied after the
+// plain bounce-back pull: the same expression as pull_one's.
+template <int Q, int FC>
+__device__ __forceinline__ void zface_wws(const Geom &g, const float *__restrict__ face_rho,
+                                          int x, int y, int z, float f[Q]) {
+  using V = VSet<Q>;
+  const float rho_t = face_rho[plane_index(g, FC, x, y, z)];
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ez = V::ez(i);
+    if constexpr ((FC == 4 && ez > 0) || (FC == 5 && ez < 0)) {
+      const float eu = (float)V::ex(i) * g.uw[FC][0] + (float)V::ey(i) * g.uw[FC][1] +
+                       (float)ez * g.uw[FC][2];
+      f[i] = f[i] - 2.f * (rho_t * V::w(i)) * eu * g.inv_cs2;
+    }
+  });
+}
+
+// Pull of one node of an interior row (x, y not on a face): every source is
+// in row (x - ex, y - ey) except where the z face rule applies, which is
+// chosen by a select on the address (no branch, so all Q loads issue
+// together).
+template <int Q, int S>
+__device__ __forceinline__ void pull_row_node(const StepArgs &a, unsigned idx, int x, int y,
+                                              int z, float f[Q]) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  const bool bottom = z == 0, top = z == a.g.nz - 1;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ez = V::ez(i);
+    const T *ps = static_cast<const T *>(a.p.src[i]) + idx;
+    if constexpr (ez == 0) {
+      f[i] = St::work(ps);
+    } else if constexpr (ez > 0) {
+      f[i] = St::work(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx : ps - 1);
+    } else {
+      f[i] = St::work(top ? static_cast<const T *>(a.p.zhi[i]) + idx : ps + 1);
+    }
+  });
+  if (bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, z, f);
+  if (top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, z, f);
 }
 
 // One node per thread, nodes in memory order so that each warp owns one
-// 32-node chunk.  Interior nodes pull with constant offsets; face nodes take
-// the face rules.  FORCE adds cul_equ2 and the second moment pass; without it
-// both are exact no-ops (the reference adds zeros and recomputes identical
-// moments), so they are skipped.
+// 32-node chunk.  Rows with interior (x, y) pull through pull_row_node;
+// rows on an x / y face take the general face rules.  FORCE adds cul_equ2
+// and the second moment pass; without it both are exact no-ops (the
+// reference adds zeros and recomputes identical moments), so they are
+// skipped.
 template <int Q, int S, bool FORCE>
 __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsigned idx) {
   using St = Storage<S>;
   using T = typename St::T;
-  using V = VSet<Q>;
   if (idx >= (unsigned)a.g.n) return;
   int x, y, z;
   a.dec(idx, x, y, z);
-  const bool face = on_any_face(a.g, x, y, z);
-  const T *__restrict__ fa = static_cast<const T *>(a.fa);
+  const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   float f[Q];
-  if (!face)
-    pull_interior<Q, S>(fa, a.g, idx, f);
+  if (row_in)
+    pull_row_node<Q, S>(a, idx, x, y, z, f);
   else
-    pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
-  finish_node<Q, FORCE>(a, f, idx, x, y, z, face);
+    pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, a.face_rho_in, f);
+  unsigned bad = 0;
+  finish_node<Q, FORCE, St::kDev>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1, bad);
+  report_bad(a.status, bad);
   if (a.fb != nullptr) {
-    T *__restrict__ fb = static_cast<T *>(a.fb);
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      St::store(fb + (long long)i * a.g.n + idx, f[i], V::w(i));
+      St::put(static_cast<T *>(a.p.dst[i]) + idx, f[i]);
     });
   }
 }
@@ -118,30 +208,14 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 
 // ---------------------------------------------------------------------------
 // Vectorised fused step: thread = NZ consecutive nodes of one z-row (nz a
-// multiple of NZ), populations moved as NZ-element vectors (16 / 8 byte
+// multiple of NZ), populations moved as NZ-element vectors (16 / 8 / 4 byte
 // loads and stores).  For rows whose (x, y) is interior every source of
 // direction i lies in row (x - ex, y - ey): one aligned vector load gives
 // NZ - |ez| of the NZ values, one scalar load the remaining one -- from the
 // neighbouring vector, or at z = 0 / z = nz - 1 from the bottom / top face
-// rule.  Rows on an x / y face take the per-node face rules.
+// rule, picked by an address select so that all loads issue together.
+// Rows on an x / y face take the per-node face rules.
 // ---------------------------------------------------------------------------
-template <int Q, int S, int NZ>
-__device__ __forceinline__ float zface_value(const typename Storage<S>::T *__restrict__ fa,
-                                             const Geom &g, int i, int rev, float w, long long row,
-                                             int fc, int x, int y, int z,
-                                             const float *__restrict__ face_rho, float eu) {
-  const int code = g.face[fc];
-  if (code == LBM_BC_PERIODICAL) {
-    // z moved to the opposite plane, same x and y
-    const int zs = (fc == 4) ? g.nz - 1 : 0;
-    return Storage<S>::load(fa + (long long)i * g.n + row + zs, w);
-  }
-  float v = Storage<S>::load(fa + (long long)rev * g.n + row + z, w);
-  if (code == LBM_BC_WALL_WITH_SPEED)
-    v -= 2.f * (face_rho[plane_index(g, fc, x, y, z)] * w) * eu * g.inv_cs2;
-  return v;
-}
-
 template <int Q, int S, bool FORCE, int NZ>
 __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned t) {
   using St = Storage<S>;
@@ -152,18 +226,15 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   if (idx0 >= (unsigned)a.g.n) return;
   int x, y, z0;
   a.dec(idx0, x, y, z0);
-  const T *__restrict__ fa = static_cast<const T *>(a.fa);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   float f[NZ][Q];
   if (row_in) {
-    const long long row = (long long)idx0 - z0;
     const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      constexpr int ex = V::ex(i), ey = V::ey(i), ez = V::ez(i);
-      constexpr float w = V::w(i);
-      const long long src = (long long)i * a.g.n + idx0 - ((long long)ex * a.g.nyz + (long long)ey * a.g.nz);
-      const Words<kWords> raw = ld_words<kWords>(fa + src);
+      constexpr int ez = V::ez(i);
+      const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
+      const Words<kWords> raw = ld_words<kWords>(ps);
       float v[NZ];
       if constexpr (St::kBits == 32) {
 #pragma unroll
@@ -171,59 +242,56 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
       } else {
 #pragma unroll
         for (int k = 0; k < NZ / 2; ++k) {
-          const float2 p2 = unpack2<S>(raw.w[k], w);
+          const float2 p2 = work2<S>(raw.w[k]);
           v[2 * k] = p2.x;
           v[2 * k + 1] = p2.y;
         }
       }
-      if (ez == 0) {
+      if constexpr (ez == 0) {
 #pragma unroll
         for (int k = 0; k < NZ; ++k) f[k][i] = v[k];
-      } else if (ez > 0) {
+      } else if constexpr (ez > 0) {
 #pragma unroll
         for (int k = 1; k < NZ; ++k) f[k][i] = v[k - 1];
-        if (bottom) {
-          const float eu = (float)ex * a.g.uw[4][0] + (float)ey * a.g.uw[4][1] + (float)ez * a.g.uw[4][2];
-          f[0][i] = zface_value<Q, S, NZ>(fa, a.g, i, V::rev(i), w, row, 4, x, y, 0, a.face_rho_in, eu);
-        } else {
-          f[0][i] = St::load(fa + src - 1, w);
-        }
+        f[0][i] = St::work(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx0 : ps - 1);
       } else {
 #pragma unroll
         for (int k = 0; k < NZ - 1; ++k) f[k][i] = v[k + 1];
-        if (top) {
-          const float eu = (float)ex * a.g.uw[5][0] + (float)ey * a.g.uw[5][1] + (float)ez * a.g.uw[5][2];
-          f[NZ - 1][i] = zface_value<Q, S, NZ>(fa, a.g, i, V::rev(i), w, row, 5, x, y, a.g.nz - 1,
-                                               a.face_rho_in, eu);
-        } else {
-          f[NZ - 1][i] = St::load(fa + src + NZ, w);
-        }
+        f[NZ - 1][i] =
+            St::work(top ? static_cast<const T *>(a.p.zhi[i]) + (idx0 + NZ - 1) : ps + NZ);
       }
     });
+    if (bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
+      zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f[0]);
+    if (top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
+      zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, a.g.nz - 1, f[NZ - 1]);
   } else {
+    const T *fa = static_cast<const T *>(a.fa);
 #pragma unroll
-    for (int k = 0; k < NZ; ++k) pull_general<Q, S>(fa, a.g, x, y, z0 + k, a.face_rho_in, f[k]);
+    for (int k = 0; k < NZ; ++k)
+      pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, a.face_rho_in, f[k]);
   }
 
+  unsigned bad = 0;
 #pragma unroll
   for (int k = 0; k < NZ; ++k) {
     const int z = z0 + k;
-    finish_node<Q, FORCE>(a, f[k], idx0 + k, x, y, z, !row_in || z == 0 || z == a.g.nz - 1);
+    finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z,
+                                    !row_in || z == 0 || z == a.g.nz - 1, bad);
   }
+  report_bad(a.status, bad);
   if (a.fb == nullptr) return;
-  T *__restrict__ fb = static_cast<T *>(a.fb);
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    constexpr float w = V::w(i);
     Words<kWords> raw;
     if constexpr (St::kBits == 32) {
 #pragma unroll
       for (int k = 0; k < NZ; ++k) raw.w[k] = __float_as_uint(f[k][i]);
     } else {
 #pragma unroll
-      for (int k = 0; k < NZ / 2; ++k) raw.w[k] = pack2<S>(f[2 * k][i], f[2 * k + 1][i], w);
+      for (int k = 0; k < NZ / 2; ++k) raw.w[k] = put2<S>(f[2 * k][i], f[2 * k + 1][i]);
     }
-    st_words(fb + (long long)i * a.g.n + idx0, raw);
+    st_words(static_cast<T *>(a.p.dst[i]) + idx0, raw);
   });
 }
 
@@ -278,6 +346,7 @@ __global__ void __launch_bounds__(TB)
   }
 }
 
+
 // ---------------------------------------------------------------------------
 // TMA-staged persistent step.  Each CTA walks groups of R whole z-rows
 // (row = (x, y)); for a row with interior (x, y) the source of direction i is
@@ -303,22 +372,23 @@ struct TmaPlan {
   long long groups;
 };
 
+// working value(s) of one / two staged elements
 template <int S>
-__device__ __forceinline__ float sm_elem(const typename Storage<S>::T *p, float w) {
+__device__ __forceinline__ float sm_elem(const typename Storage<S>::T *p) {
   if constexpr (Storage<S>::kBits == 32)
     return *p;
   else if constexpr (S == LBM_STORAGE_FP16S)
-    return w + __half2float(*p);
+    return __half2float(*p);
   else
-    return w + __bfloat162float(*p);
+    return __bfloat162float(*p);
 }
 
 template <int S>
-__device__ __forceinline__ float2 sm_pair(const typename Storage<S>::T *p, float w) {
+__device__ __forceinline__ float2 sm_pair(const typename Storage<S>::T *p) {
   if constexpr (Storage<S>::kBits == 32)
     return *reinterpret_cast<const float2 *>(p);
   else
-    return unpack2<S>(*reinterpret_cast<const unsigned *>(p), w);
+    return work2<S>(*reinterpret_cast<const unsigned *>(p));
 }
 
 template <int Q, int S, bool FORCE>
@@ -402,54 +472,44 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
       const bool row_in = interior(x, y);
       if (row_in) {
         const T *srow = buf + (long long)(s * R + j) * Q * nz;
-        const long long row = r * nz;
         static_for<Q>([&](auto ic) {
           constexpr int i = decltype(ic)::value;
           constexpr int ez = V::ez(i);
-          constexpr float w = V::w(i);
           const T *rp = srow + (long long)i * nz;
           if constexpr (ez == 0) {
-            const float2 v = sm_pair<S>(rp + z, w);
+            const float2 v = sm_pair<S>(rp + z);
             f0[i] = v.x;
             f1[i] = v.y;
           } else if constexpr (ez > 0) {
-            f1[i] = sm_elem<S>(rp + z, w);
-            if (z == 0) {
-              const float eu = (float)V::ex(i) * a.g.uw[4][0] + (float)V::ey(i) * a.g.uw[4][1] +
-                               (float)ez * a.g.uw[4][2];
-              f0[i] = zface_value<Q, S, 2>(fa, a.g, i, V::rev(i), w, row, 4, x, y, 0,
-                                           a.face_rho_in, eu);
-            } else {
-              f0[i] = sm_elem<S>(rp + z - 1, w);
-            }
+            f1[i] = sm_elem<S>(rp + z);
+            f0[i] = z == 0 ? St::work(static_cast<const T *>(a.p.zlo[i]) + idx)
+                           : sm_elem<S>(rp + z - 1);
           } else {
-            f0[i] = sm_elem<S>(rp + z + 1, w);
-            if (z + 2 == nz) {
-              const float eu = (float)V::ex(i) * a.g.uw[5][0] + (float)V::ey(i) * a.g.uw[5][1] +
-                               (float)ez * a.g.uw[5][2];
-              f1[i] = zface_value<Q, S, 2>(fa, a.g, i, V::rev(i), w, row, 5, x, y, nz - 1,
-                                           a.face_rho_in, eu);
-            } else {
-              f1[i] = sm_elem<S>(rp + z + 2, w);
-            }
+            f0[i] = sm_elem<S>(rp + z + 1);
+            f1[i] = z + 2 == nz ? St::work(static_cast<const T *>(a.p.zhi[i]) + (idx + 1))
+                                : sm_elem<S>(rp + z + 2);
           }
         });
+        if (z == 0 && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
+          zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f0);
+        if (z + 2 == nz && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
+          zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, nz - 1, f1);
       } else {
-        pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f0);
-        pull_general<Q, S>(fa, a.g, x, y, z + 1, a.face_rho_in, f1);
+        pull_general<Q, S, true>(fa, a.g, x, y, z, a.face_rho_in, f0);
+        pull_general<Q, S, true>(fa, a.g, x, y, z + 1, a.face_rho_in, f1);
       }
-      finish_node<Q, FORCE>(a, f0, idx, x, y, z, !row_in || z == 0);
-      finish_node<Q, FORCE>(a, f1, idx + 1, x, y, z + 1, !row_in || z + 1 == nz - 1);
+      unsigned bad = 0;
+      finish_node<Q, FORCE, St::kDev>(a, f0, idx, x, y, z, !row_in || z == 0, bad);
+      finish_node<Q, FORCE, St::kDev>(a, f1, idx + 1, x, y, z + 1, !row_in || z + 1 == nz - 1, bad);
+      report_bad(a.status, bad);
       if (a.fb != nullptr) {
-        T *__restrict__ fb = static_cast<T *>(a.fb);
         static_for<Q>([&](auto ic) {
           constexpr int i = decltype(ic)::value;
-          constexpr float w = V::w(i);
-          T *dst = fb + (long long)i * a.g.n + idx;
+          T *dst = static_cast<T *>(a.p.dst[i]) + idx;
           if constexpr (St::kBits == 32)
             *reinterpret_cast<float2 *>(dst) = make_float2(f0[i], f1[i]);
           else
-            *reinterpret_cast<unsigned *>(dst) = pack2<S>(f0[i], f1[i], w);
+            *reinterpret_cast<unsigned *>(dst) = put2<S>(f0[i], f1[i]);
         });
       }
     }
