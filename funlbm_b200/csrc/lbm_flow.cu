@@ -424,12 +424,12 @@ int lbm_batch_pack(const lbm_lattice *lat, const void *fa, void *fb, const lbm_f
                            use_force, "lbm_batch_pack");
   if (rc) return rc;
   const int bits = lat->storage == LBM_STORAGE_FP32 ? 32 : 16;
-  if (nodes != 1 && !(nodes == 2 && step_shape_ok(2, lat->nz, bits))) {
-    set_error("lbm_batch_pack: nodes per thread must be 1, or 2 for rows of an even number "
-              "(>= 4) of nodes");
+  if (nodes != 1 && !((nodes == 2 || nodes == 4) && step_shape_ok(nodes, lat->nz, bits))) {
+    set_error("lbm_batch_pack: nodes per thread must be 1, or 2 / 4 for rows of a multiple of "
+              "that many nodes (at least twice as many)");
     return LBM_ERR_INVALID;
   }
-  const long long per_block = (nodes == 2 ? 128 : 256) * (long long)kBatchTiles;
+  const long long per_block = (nodes == 1 ? 256 : 128) * (long long)kBatchTiles;
   const long long work = a.g.n / nodes;
   *blocks = (uint32_t)((work + per_block - 1) / per_block);
   memcpy(entry, &a, sizeof(a));
@@ -443,8 +443,8 @@ int lbm_flow_step_batch(int32_t q, int32_t storage, int32_t nodes, int32_t force
     set_error("lbm_flow_step_batch: empty batch");
     return LBM_ERR_INVALID;
   }
-  if (nodes != 1 && nodes != 2) {
-    set_error("lbm_flow_step_batch: nodes per thread must be 1 or 2");
+  if (nodes != 1 && nodes != 2 && nodes != 4) {
+    set_error("lbm_flow_step_batch: nodes per thread must be 1, 2 or 4");
     return LBM_ERR_INVALID;
   }
   const StepArgs *e = static_cast<const StepArgs *>(entries);

@@ -126,6 +126,8 @@ struct Storage<LBM_STORAGE_FP32> {
   using T = float;
   static constexpr int kBits = 32;
   static constexpr bool kDev = false;
+  __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
+  __device__ __forceinline__ static float cvt(T v) { return v; }
   __device__ __forceinline__ static float work(const T *p) { return __ldg(p); }
   __device__ __forceinline__ static void put(T *p, float v) { *p = v; }
   __device__ __forceinline__ static float load(const T *p, float) { return __ldg(p); }
@@ -138,6 +140,8 @@ struct Storage<LBM_STORAGE_FP16S> {
   using T = __half;
   static constexpr int kBits = 16;
   static constexpr bool kDev = true;
+  __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
+  __device__ __forceinline__ static float cvt(T v) { return __half2float(v); }
   __device__ __forceinline__ static float work(const T *p) { return __half2float(__ldg(p)); }
   __device__ __forceinline__ static void put(T *p, float v) { *p = __float2half_rn(v); }
   __device__ __forceinline__ static float load(const T *p, float w) {
@@ -158,6 +162,8 @@ struct Storage<LBM_STORAGE_BF16S> {
   using T = __nv_bfloat16;
   static constexpr int kBits = 16;
   static constexpr bool kDev = true;
+  __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
+  __device__ __forceinline__ static float cvt(T v) { return __bfloat162float(v); }
   __device__ __forceinline__ static float work(const T *p) { return __bfloat162float(__ldg(p)); }
   __device__ __forceinline__ static void put(T *p, float v) { *p = __float2bfloat16_rn(v); }
   __device__ __forceinline__ static float load(const T *p, float w) {

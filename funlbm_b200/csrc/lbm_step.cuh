@@ -216,11 +216,95 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 // rule, picked by an address select so that all loads issue together.
 // Rows on an x / y face take the per-node face rules.
 // ---------------------------------------------------------------------------
+// 16-bit storage: the vectors stay packed in registers and are unpacked one
+// node pair at a time, right before that pair is finished and stored (one
+// 32-bit word per direction), so a thread holds 2 x Q floats instead of
+// NZ x Q.  Measured on B200 it is the faster form for 2 nodes per thread
+// (fewer registers, more resident warps); for 4 and 8 the fully unpacked
+// form below keeps more independent work per thread and wins.  Same
+// arithmetic per node as every other shape.
+template <int Q, int S, bool FORCE, int NZ>
+__device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned t) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  static_assert(St::kBits == 16 && NZ % 2 == 0, "pairs of 16-bit elements");
+  constexpr int kWords = NZ / 2;
+  const unsigned idx0 = t * NZ;
+  if (idx0 >= (unsigned)a.g.n) return;
+  int x, y, z0;
+  a.dec(idx0, x, y, z0);
+  const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
+  const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
+  Words<kWords> raw[Q];
+  T extra[Q];
+  if (row_in) {
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int ez = V::ez(i);
+      const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
+      raw[i] = ld_words<kWords>(ps);
+      if constexpr (ez > 0)
+        extra[i] = St::raw(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx0 : ps - 1);
+      if constexpr (ez < 0)
+        extra[i] = St::raw(top ? static_cast<const T *>(a.p.zhi[i]) + (idx0 + NZ - 1) : ps + NZ);
+    });
+  }
+  unsigned bad = 0;
+#pragma unroll
+  for (int pr = 0; pr < kWords; ++pr) {
+    float f0[Q], f1[Q];
+    const int za = z0 + 2 * pr;
+    if (row_in) {
+      static_for<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        constexpr int ez = V::ez(i);
+        const float2 v = work2<S>(raw[i].w[pr]);
+        if constexpr (ez == 0) {
+          f0[i] = v.x;
+          f1[i] = v.y;
+        } else if constexpr (ez > 0) {
+          f0[i] = pr == 0 ? St::cvt(extra[i]) : work2<S>(raw[i].w[pr > 0 ? pr - 1 : 0]).y;
+          f1[i] = v.x;
+        } else {
+          f0[i] = v.y;
+          f1[i] = pr == kWords - 1 ? St::cvt(extra[i])
+                                   : work2<S>(raw[i].w[pr < kWords - 1 ? pr + 1 : pr]).x;
+        }
+      });
+      if (pr == 0 && bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
+        zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f0);
+      if (pr == kWords - 1 && top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
+        zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, a.g.nz - 1, f1);
+    } else {
+      const T *fa = static_cast<const T *>(a.fa);
+      pull_general<Q, S, true>(fa, a.g, x, y, za, a.face_rho_in, f0);
+      pull_general<Q, S, true>(fa, a.g, x, y, za + 1, a.face_rho_in, f1);
+    }
+    finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
+                                !row_in || za == 0 || za == a.g.nz - 1, bad);
+    finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
+                                !row_in || za + 1 == 0 || za + 1 == a.g.nz - 1, bad);
+    if (a.fb != nullptr) {
+      static_for<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        st_words(static_cast<T *>(a.p.dst[i]) + idx0 + 2 * pr,
+                 Words<1>{{put2<S>(f0[i], f1[i])}});
+      });
+    }
+  }
+  report_bad(a.status, bad);
+}
+
 template <int Q, int S, bool FORCE, int NZ>
 __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned t) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
+  if constexpr (St::kBits == 16 && NZ == 2) {
+    step_vec_pairs<Q, S, FORCE, NZ>(a, t);
+    return;
+  }
   constexpr int kWords = NZ * St::kBits / 32;
   const unsigned idx0 = t * NZ;
   if (idx0 >= (unsigned)a.g.n) return;
@@ -295,8 +379,25 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   });
 }
 
+// Register cap of the vectorised step for 16-bit storage, as resident blocks
+// per SM asked of the compiler (0 = no cap).  A 16-bit population costs a
+// whole float register once unpacked, so without a cap the 4-node 16-bit
+// kernels of D3Q15 / D3Q19 hold too few bytes in flight per SM to cover HBM
+// latency; the cap (measured on B200 at 512^3) trades a few spilled words
+// for a third more resident warps.  FP32 runs uncapped.
+template <int Q, int S, int NZ>
+constexpr int vec_reg_cap() {
+  if (Storage<S>::kBits == 32) return 0;
+  if (NZ == 4) return Q == 15 || Q == 19 ? 128 : 0;
+  return 0;
+}
+template <int Q, int S, int NZ, int TB>
+constexpr int vec_min_blocks() {
+  return vec_reg_cap<Q, S, NZ>() == 0 ? 0 : 65536 / (vec_reg_cap<Q, S, NZ>() * TB);
+}
+
 template <int Q, int S, bool FORCE, int NZ, int TB>
-__global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
+__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB>())) k_step_vec(const StepArgs a) {
   step_vec_body<Q, S, FORCE, NZ>(a, blockIdx.x * TB + threadIdx.x);
 }
 
@@ -312,7 +413,7 @@ __global__ void __launch_bounds__(TB) k_step_vec(const StepArgs a) {
 constexpr int kBatchTiles = 4;   // tiles of TB threads per block (amortises the lookup)
 
 template <int Q, int S, bool FORCE, int NZ, int TB>
-__global__ void __launch_bounds__(TB)
+__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB>()))
     k_step_batch(const StepArgs *__restrict__ entries, const unsigned *__restrict__ block_begin,
                  int count) {
   __shared__ __align__(16) StepArgs sa;
@@ -633,9 +734,12 @@ struct StepLauncher {
     constexpr int bits = Storage<S>::kBits;
     if (nodes == LBM_STEP_ROWS) return go_tma(a, force, s);
     if (nodes == 0) {
-      // measured on B200: 2 nodes per thread with 128-thread blocks is the
-      // fastest shape for every velocity set in float32 (see funlbm_b200.tune)
-      nodes = step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
+      // measured on B200 at 512^3: 2 nodes per thread with 128-thread blocks
+      // is the fastest shape for every velocity set and storage, except
+      // D3Q19 in 16-bit storage, where 4 nodes per thread (register-capped)
+      // are (see funlbm_b200.tune)
+      const int want = (bits == 16 && Q == 19) ? 4 : 2;
+      nodes = step_shape_ok(want, a.g.nz, bits) ? want : step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
       threads = threads ? threads : 128;
     }
     if (nodes == 2) {
@@ -662,7 +766,7 @@ struct StepLauncher {
 };
 
 // Multi-lattice launch for velocity set Q and storage S: nodes per thread 1
-// (256 threads) or 2 (128 threads).
+// (256 threads), 2 or 4 (128 threads).
 template <int Q, int S>
 int run_step_batch_qs(const StepArgs *entries, const unsigned *block_begin, int count,
                       unsigned total_blocks, bool force, int nodes, cudaStream_t s) {
@@ -671,6 +775,11 @@ int run_step_batch_qs(const StepArgs *entries, const unsigned *block_begin, int 
       k_step_batch<Q, S, true, 2, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
     else
       k_step_batch<Q, S, false, 2, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
+  } else if (nodes == 4) {
+    if (force)
+      k_step_batch<Q, S, true, 4, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
+    else
+      k_step_batch<Q, S, false, 4, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
   } else {
     if (force)
       k_step_batch<Q, S, true, 1, 256><<<total_blocks, 256, 0, s>>>(entries, block_begin, count);

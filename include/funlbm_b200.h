@@ -142,8 +142,9 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
  * the exclusive prefix sum of their block counts to device memory, and
  * launches.  A lattice's result is the same in a batch as alone. */
 size_t lbm_batch_entry_bytes(void);
-/* nodes: 1 (one node per thread) or 2 (two z-nodes per thread; rows of an
- * even number >= 4 of nodes).  *blocks receives the lattice's block count. */
+/* nodes: 1 (one node per thread), 2 or 4 (that many z-nodes per thread; rows
+ * of a multiple of that many nodes, at least twice as many).  *blocks
+ * receives the lattice's block count. */
 int lbm_batch_pack(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
                    const float *face_rho_in, float *face_rho_out, uint32_t *status, int32_t nodes,
                    void *entry, uint32_t *blocks);
