@@ -31,6 +31,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# one hardware queue per stream of the serving pool (read when CUDA starts)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 Q = 19
 TAU_MU = 1.0 / 30.0
@@ -55,8 +57,8 @@ def parse():
     ap.add_argument("--cpu-size", type=int, default=64)
     ap.add_argument("--serve", action="store_true",
                     help="run the served-stream benchmark and print its own line")
-    ap.add_argument("--serve-requests", type=int, default=64)
-    ap.add_argument("--serve-steps", type=int, nargs=2, default=[100, 600])
+    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=[500, 5000])
     ap.add_argument("--serve-budget", type=float, default=160e9)
     ap.add_argument("--serve-mode", default="streams", choices=["streams", "batched"])
     ap.add_argument("--serve-particles", type=int, default=1,
@@ -388,11 +390,13 @@ def run_serve(args):
             r.config["particles"] = []
     work = sum(r.steps * np.prod([d + 1 for d in r.config["flow"]["size"]]) for r in base)
 
-    # sequential: each request alone through the plain path
+    # sequential: each request alone through the plain FP32 path
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r in base:
-        lbm = LBMD3(config=Config().from_json(copy.deepcopy(r.config)))
+        cfg = copy.deepcopy(r.config)
+        cfg["flow"]["precision"]["storage"] = "fp32"
+        lbm = LBMD3(config=Config().from_json(cfg))
         lbm.init()
         for _ in range(r.steps):
             lbm.run_step(step=lbm.step)
@@ -435,7 +439,8 @@ def run_serve(args):
                     "aggregate_mlups": work / poi_s / 1e6},
         "budget_gb": args.serve_budget / 1e9, "mode": args.serve_mode,
         "stats_saturated": stats_sat,
-        "note": "sequential = each request alone through LBMD3.run_step (plain fused path)",
+        "note": "sequential = each request alone through LBMD3.run_step with FP32 storage "
+                "(the plain path); served = each request in its own storage (fp32 / fp16s)",
     }
 
 

@@ -85,18 +85,24 @@ class _Slot:
         self.remaining = req.steps
         self.started = False
         self.stream = None
-        self.graphs = []
-        self.done = None
+        self.graphs = {}
+        self.inflight = []
 
 
 class LBMServer:
     """Continuous-batching server of LBM solves on one GPU.
 
-    mode="streams" (default): every admitted request gets a stream from a
-    pool and its own CUDA graphs of up to `graph_steps` steps (captured
-    without a device synchronisation); its whole run is enqueued at
-    admission and overlaps on the device with the others.  Completion is polled with events, so
-    finishing or admitting a request never stalls the rest.
+    mode="streams" (default): every admitted request gets the least-loaded
+    stream of a pool and its own CUDA graphs of up to `graph_steps` steps.
+    Its run is enqueued in chunks of `chunk_steps` steps, at most two chunks
+    ahead of the device, so the requests' work overlaps on the GPU while no
+    stream holds a long backlog.  Everything that synchronises with the host
+    (building the request, its first step, graph capture, reading results)
+    runs on a separate, lightly loaded init stream, and completion is polled
+    with events, so admitting or finishing a request never waits for the
+    others' work.  Run the process with CUDA_DEVICE_MAX_CONNECTIONS=32 (set
+    before CUDA starts) so that the pool's streams do not share hardware
+    queues.
 
     mode="batched": all active lattices of one (velocity set, storage, nodes
     per thread) advance together in one multi-lattice step launch per step;
@@ -105,12 +111,16 @@ class LBMServer:
     """
 
     def __init__(self, budget_bytes=160e9, max_slots=256, device="cuda", use_graphs=True,
-                 chunk=32, mode="streams", streams=32, graph_steps=64):
+                 chunk=32, mode="streams", streams=31, graph_steps=32, chunk_steps=256,
+                 reserve=True, tune=True):
         if mode not in ("streams", "batched"):
             raise ValueError("mode must be 'streams' or 'batched'")
         self.mode = mode
+        self.tune = bool(tune)
         self.graph_steps = max(2, int(graph_steps) - int(graph_steps) % 2)
+        self.chunk_steps = max(self.graph_steps, int(chunk_steps))
         self._streams = [torch.cuda.Stream(device=device) for _ in range(max(1, int(streams)))]
+        self._init_stream = torch.cuda.Stream(device=device)
         self._next_stream = 0
         self.budget = int(budget_bytes)
         self.max_slots = int(max_slots)
@@ -127,6 +137,18 @@ class LBMServer:
         self.stats = {"graph_captures": 0, "graph_replays": 0, "eager_steps": 0,
                       "batched_launches": 0, "max_active": 0, "max_used_bytes": 0,
                       "t_admit": 0.0, "t_capture": 0.0, "t_steps": 0.0, "t_retire": 0.0}
+        if reserve:
+            self._reserve_memory()
+
+    def _reserve_memory(self):
+        """Have the caching allocator take the budget from the device once, up
+        front: later allocations are carved out of that cached segment instead
+        of calling cudaMalloc, which stalls the host while the GPU is busy."""
+        free, _ = torch.cuda.mem_get_info(self.device)
+        nbytes = min(self.budget, free - (2 << 30))
+        if nbytes > 0:
+            block = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            del block
 
     # -- queue ---------------------------------------------------------------
     def submit(self, req: Request):
@@ -154,14 +176,22 @@ class LBMServer:
             cfg.setdefault("file", {"per_steps": 10 ** 9})
             cfg["device"] = str(self.device)
             if self.mode == "streams":
-                stream = self._streams[self._next_stream % len(self._streams)]
-                self._next_stream += 1
-                with torch.cuda.stream(stream):
+                init = self._init_stream
+                with torch.cuda.stream(init):
                     lbm = LBMD3(config=Config().from_json(cfg))
                     lbm.init()
                     slot = _Slot(req, lbm, nbytes)
-                    slot.stream = stream
-                    self._enqueue_run(slot)
+                    # the first step enters the fused representation (allocates)
+                    lbm.run_step(step=lbm.step)
+                    lbm.step += 1
+                    slot.remaining -= 1
+                    self.stats["eager_steps"] += 1
+                    self._tune(lbm)
+                    ready = torch.cuda.Event()
+                    ready.record(init)
+                slot.stream = self._pick_stream()
+                slot.stream.wait_event(ready)
+                self._top_up(slot)
             else:
                 lbm = LBMD3(config=Config().from_json(cfg))
                 lbm.init()
@@ -175,68 +205,103 @@ class LBMServer:
         self.stats["max_used_bytes"] = max(self.stats["max_used_bytes"], self.used)
         return admitted
 
+    def _tune(self, lbm):
+        """Launch shape of this request's step kernel from the autotuner (per
+        class of lattice, cached), before any graph captures it."""
+        if not self.tune:
+            return
+        from .tune import tune_class
+
+        lat = lbm.flow.lattice
+        if lat is not None and lat.fused:
+            forced = bool(lbm.particle_swarm.particles) or lbm.body_force != (0, 0, 0)
+            tune_class(lat, forced=forced)
+
     # -- streams mode --------------------------------------------------------------
-    def _capture_steps(self, lbm, stream, n):
-        """Capture n (even) fused steps of one lattice on `stream` (no device
-        sync; nothing runs).  The bookkeeping returns to the same buffers after
-        an even number of steps, so the graph can be replayed any number of
-        times."""
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.stream(stream):
-            g.capture_begin()
-            try:
-                for _ in range(n):
-                    lbm._fused_step()
-            finally:
-                g.capture_end()
-        self.stats["graph_captures"] += 1
+    def _pick_stream(self):
+        load = {id(st): 0 for st in self._streams}
+        for slot in self.active:
+            if slot.stream is not None:
+                load[id(slot.stream)] += 1
+        return min(self._streams, key=lambda st: load[id(st)])
+
+    def _graph_for(self, slot, n):
+        """The captured n-step graph of this lattice for its current buffer
+        parity and interpolation phase (the weight-sum check switches on after
+        step 100, lbm/lbm3d.py:84, and is a parameter of the captured
+        launches); captured on the init stream the first time it is needed
+        (no device synchronisation; nothing runs).  The bookkeeping returns to
+        the same buffers after an even number of steps, so a graph can be
+        replayed any number of times."""
+        lbm = slot.lbm
+        key = (n, lbm.step > 100, lbm.flow.lattice.cur, getattr(lbm, "_fi", 0))
+        g = slot.graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(self._init_stream):
+                g.capture_begin()
+                try:
+                    for _ in range(n):
+                        lbm._fused_step()
+                finally:
+                    g.capture_end()
+            slot.graphs[key] = g
+            self.stats["graph_captures"] += 1
         return g
 
-    def _enqueue_run(self, slot):
-        """Enqueue the whole run of one request on its stream: the first step
-        eagerly (it enters the fused representation and allocates), then
-        replays of captured graphs of up to `graph_steps` steps -- separate
-        graphs for steps up to 100 and after, because the interpolation's
-        weight-sum check (active after step 100, lbm/lbm3d.py:84) is a
-        parameter of the captured launches -- and eager steps for what is
-        left over."""
-        lbm, rem = slot.lbm, slot.remaining
-        s = slot.stream
-        with torch.cuda.stream(s):
-            lbm.run_step(step=lbm.step)
-            lbm.step += 1
-            rem -= 1
-            self.stats["eager_steps"] += 1
-            while rem > 0:
-                if self.use_graphs and rem >= 2:
-                    span = rem if lbm.step > 100 else min(rem, 101 - lbm.step)
-                    n = min(self.graph_steps, span)
-                    n -= n % 2
-                    if n >= 2:
-                        reps = span // n
-                        g = self._capture_steps(lbm, s, n)
-                        slot.graphs.append(g)
-                        for _ in range(reps):
-                            g.replay()
-                        self.stats["graph_replays"] += reps
-                        lbm.step += n * reps
-                        rem -= n * reps
-                        continue
-                lbm.run_step(step=lbm.step)
-                lbm.step += 1
-                rem -= 1
-                self.stats["eager_steps"] += 1
-            slot.done = torch.cuda.Event()
-            slot.done.record(s)
-        slot.remaining = 0
+    def _top_up(self, slot):
+        """Keep up to two chunks of `chunk_steps` steps of this request
+        enqueued on its stream: graph replays (separate graphs for steps up to
+        100 and after) and eager steps for an odd remainder."""
+        lbm = slot.lbm
+        while len(slot.inflight) < 2 and slot.remaining > 0:
+            budget = self.chunk_steps
+            with torch.cuda.stream(slot.stream):
+                while budget > 0 and slot.remaining > 0:
+                    rem = slot.remaining
+                    if self.use_graphs and rem >= 2 and budget >= 2:
+                        span = rem if lbm.step > 100 else min(rem, 101 - lbm.step)
+                        n = min(self.graph_steps, span, budget)
+                        n -= n % 2
+                        if n >= 2:
+                            g = self._graph_for(slot, n)
+                            reps = max(1, min(span, budget) // n)
+                            for _ in range(reps):
+                                g.replay()
+                            self.stats["graph_replays"] += reps
+                            lbm.step += n * reps
+                            slot.remaining -= n * reps
+                            budget -= n * reps
+                            continue
+                    lbm.run_step(step=lbm.step)
+                    lbm.step += 1
+                    slot.remaining -= 1
+                    budget -= 1
+                    self.stats["eager_steps"] += 1
+                ev = torch.cuda.Event()
+                ev.record(slot.stream)
+            slot.inflight.append(ev)
+
+    def _pump_streams(self):
+        """Drop completed chunks and top every request up; True if anything
+        completed."""
+        progressed = False
+        for slot in self.active:
+            while slot.inflight and slot.inflight[0].query():
+                slot.inflight.pop(0)
+                progressed = True
+            if slot.remaining > 0 and len(slot.inflight) < 2:
+                self._top_up(slot)
+        return progressed
 
     def _retire_streams(self, now_fn):
-        finished = [slot for slot in self.active if slot.done is not None and slot.done.query()]
+        finished = [slot for slot in self.active if slot.remaining <= 0 and not slot.inflight]
         if not finished:
             return False
+        init = self._init_stream
         for slot in finished:
             lbm = slot.lbm
-            with torch.cuda.stream(slot.stream):
+            with torch.cuda.stream(init):
                 res = {"rho": lbm.flow.rou.clone(), "u": lbm.flow.u.clone(),
                        "status": lbm.check_status(), "steps": lbm.step - 1}
                 ps = lbm.particle_swarm.particles
@@ -244,12 +309,14 @@ class LBMServer:
                     res["cx"] = torch.stack([p.cx for p in ps]).clone()
                     res["cu"] = torch.stack([p.cu for p in ps]).clone()
                     res["cw"] = torch.stack([p.cw for p in ps]).clone()
-            slot.stream.synchronize()
+                done = torch.cuda.Event()
+                done.record(init)
+            done.synchronize()
             slot.req.result = res
             slot.req.finished_at = now_fn()
             self.used -= slot.nbytes
             self.done.append(slot.req)
-            slot.graphs = []
+            slot.graphs = {}
             slot.lbm = None
         self.active = [slot for slot in self.active if slot not in finished]
         return True
@@ -466,10 +533,13 @@ class LBMServer:
                 ta = time.perf_counter()
                 self._admit(now())
                 self.stats["t_admit"] += time.perf_counter() - ta
+                ts = time.perf_counter()
+                progressed = self._pump_streams()
                 tr = time.perf_counter()
+                self.stats["t_steps"] += tr - ts
                 retired = self._retire_streams(lambda: time.perf_counter() - t0)
                 self.stats["t_retire"] += time.perf_counter() - tr
-                if not retired:
+                if not retired and not progressed:
                     if self.queue and not self.active:
                         wait = self.queue[0].arrival - now()
                         time.sleep(min(max(wait, 0.0), 0.05))

@@ -77,5 +77,57 @@ def tune(lat, force=None, iters=6, warmup=2, verbose=False):
     return choice, timings
 
 
+_CLASS_CACHE = {}
+CLASS_PROXY_NODES = 96          # proxy lattice of a class: about 96^3 nodes
+
+
+def class_key(lat, forced):
+    nz = lat.shape[2]
+    return (lat.q, lat.storage, nz % 2 == 0 and nz >= 4, nz % 4 == 0 and nz >= 8,
+            nz % 8 == 0 and nz >= 16, bool(forced))
+
+
+def tune_class(lat, forced=False, iters=6, warmup=2):
+    """Launch shape for ``lat`` from its class -- velocity set, storage,
+    which vector widths its rows allow, forced or not -- tuned once per class
+    on a ~96^3 proxy with the lattice's faces and cached.  Meant for servers
+    that see many lattice sizes: one short tuning per class instead of one per
+    (ny, nz).  Returns the choice."""
+    from .lattice import Lattice, make_force
+
+    key = class_key(lat, forced)
+    if key not in _CLASS_CACHE:
+        _, even, by4, by8, _ = key[1:]
+        nz = 96 if by8 else 100 if by4 else 98 if even else 97
+        n = CLASS_PROXY_NODES
+        proxy = Lattice(lat.q, (n, n, nz), lat.faces, lat.tau, storage=lat.storage,
+                        face_uw=lat.face_uw, re_mu=lat.re_mu, device=lat.device)
+        proxy.init(None)
+        force = make_force((0, 0, 0), (1e-6, 0, 0)) if forced else None
+        bits = 32 if lat.storage == "fp32" else 16
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        timings = {}
+        for nodes, threads in CANDIDATES[bits]:
+            if nodes == ROWS or not shape_ok(nodes, nz, bits):
+                continue
+            proxy.set_launch_shape(nodes, threads)
+            for _ in range(warmup):
+                proxy.step(force)
+            start.record()
+            for _ in range(iters):
+                proxy.step(force)
+            stop.record()
+            stop.synchronize()
+            timings[(nodes, threads)] = start.elapsed_time(stop) / iters
+        proxy.release()
+        del proxy
+        _CLASS_CACHE[key] = min(timings, key=timings.get)
+    choice = _CLASS_CACHE[key]
+    lat.set_launch_shape(*choice)
+    return choice
+
+
 def clear_cache():
     _CACHE.clear()
+    _CLASS_CACHE.clear()
