@@ -15,6 +15,8 @@ void set_error(const char *fmt, ...);
 int fail_cuda(cudaError_t e, const char *where);
 int check_lattice(const lbm_lattice *lat);  // LBM_OK or an error code (message set)
 Geom make_geom(const lbm_lattice *lat);
+// pull-source / face-source / destination plane pointers of a lattice step
+void fill_step_planes(const Geom &g, int q, int storage, const void *fa, void *fb, StepPlanes &p);
 bool any_face(const lbm_lattice *lat, int code);
 
 // Launch-error check after a kernel launch.

@@ -111,6 +111,39 @@ Geom make_geom(const lbm_lattice *lat) {
   return g;
 }
 
+// Plane pointers (StepPlanes) for velocity set q, elements
+// of `elem` bytes.  Pure address arithmetic: nothing is dereferenced here.
+template <int Q>
+static void fill_planes_q(const Geom &g, const void *fa, void *fb, int elem, StepPlanes &p) {
+  using V = VSet<Q>;
+  const uintptr_t a = (uintptr_t)fa, b = (uintptr_t)fb;
+  auto at = [&](uintptr_t base, long long e) { return base + (uintptr_t)(e * elem); };
+  for (int i = 0; i < Q; ++i) {
+    const long long plane = (long long)i * g.n, rplane = (long long)V::rev(i) * g.n;
+    p.src[i] = (const void *)at(a, plane - (long long)V::ex(i) * g.nyz - (long long)V::ey(i) * g.nz);
+    p.zlo[i] = nullptr;
+    p.zhi[i] = nullptr;
+    if (V::ez(i) > 0)
+      p.zlo[i] = (const void *)(g.face[4] == LBM_BC_PERIODICAL ? at(a, plane + g.nz - 1)
+                                                               : at(a, rplane));
+    if (V::ez(i) < 0)
+      p.zhi[i] = (const void *)(g.face[5] == LBM_BC_PERIODICAL ? at(a, plane - (g.nz - 1))
+                                                               : at(a, rplane));
+    p.dst[i] = fb == nullptr ? nullptr : (void *)at(b, plane);
+  }
+}
+
+void fill_step_planes(const Geom &g, int q, int storage, const void *fa, void *fb,
+                             StepPlanes &p) {
+  const int elem = storage == LBM_STORAGE_FP32 ? 4 : 2;
+  switch (q) {
+    case 13: fill_planes_q<13>(g, fa, fb, elem, p); break;
+    case 15: fill_planes_q<15>(g, fa, fb, elem, p); break;
+    case 19: fill_planes_q<19>(g, fa, fb, elem, p); break;
+    default: fill_planes_q<27>(g, fa, fb, elem, p); break;
+  }
+}
+
 }  // namespace lbm
 
 extern "C" {

@@ -88,6 +88,7 @@ struct InterpArgs {
   float dt;
   int step;
   unsigned *status;
+  StepPlanes planes;   // pull sources of fa (interior rows)
 };
 
 template <int Q, int S>
@@ -110,7 +111,10 @@ __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
       if (a.fa != nullptr) {
         const typename Storage<S>::T *fa = static_cast<const typename Storage<S>::T *>(a.fa);
         float f[Q];
-        pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
+        if (x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1)
+          pull_row_node<Q, S, false>(a.planes, a.g, a.face_rho_in, (unsigned)idx, x, y, z, f);
+        else
+          pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
         float fx = a.go[0], fy = a.go[1], fz = a.go[2];
         if (a.fol_old != nullptr) {
           fx += a.fol_old[3 * idx];
@@ -300,21 +304,16 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
 // ---------------------------------------------------------------------------
 // Spreading (lbm/lbm3d.py:102-119)
 // ---------------------------------------------------------------------------
-// Clear the chunks written last time this buffer was used (warp per chunk).
+// Clear the chunks written last time this buffer was used: one thread per
+// chunk (only a few chunks are flagged, so most threads read one byte).
 __global__ void k_spread_clear(long long n, float *field, uint8_t *chunks) {
-  const long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+  const long long chunk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nchunks = (n + 31) >> 5;
-  if (chunk >= nchunks) return;
-  if (chunks[chunk] == 0) return;
-  const long long node = chunk * 32 + lane;
-  if (node < n) {
-    field[3 * node] = 0.f;
-    field[3 * node + 1] = 0.f;
-    field[3 * node + 2] = 0.f;
-  }
-  __syncwarp();
-  if (lane == 0) chunks[chunk] = 0;
+  if (chunk >= nchunks || chunks[chunk] == 0) return;
+  const long long first = chunk * 32;
+  const long long last = first + 32 < n ? first + 32 : n;
+  for (long long k = 3 * first; k < 3 * last; ++k) field[k] = 0.f;
+  chunks[chunk] = 0;
 }
 
 struct SpreadArgs {
@@ -521,6 +520,7 @@ int ibm_interpolate(const lbm_lattice *lat, const void *fa, const lbm_force *for
   memset(&a, 0, sizeof(a));
   a.g = make_geom(lat);
   a.fa = fa;
+  if (fa != nullptr) fill_step_planes(a.g, lat->q, lat->storage, fa, nullptr, a.planes);
   a.u_field = u_field;
   a.rho_field = rho_field;
   if (force != nullptr) {
@@ -597,7 +597,7 @@ int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, fl
   a.chunks = chunks;
   a.owner = owner;
   const long long nchunks = (a.g.n + 31) >> 5;
-  k_spread_clear<<<blocks_for(nchunks * 32, 256), 256, 0, s>>>(a.g.n, field, chunks);
+  k_spread_clear<<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, field, chunks);
   LBM_LAUNCH_CHECK("ibm_spread");
   if (pt->n_markers == 0) return LBM_OK;
   const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
@@ -656,7 +656,7 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
   a.chunks = chunks;
   a.owner = owner;
   const long long nchunks = (a.g.n + 31) >> 5;
-  k_spread_clear<<<blocks_for(nchunks * 32, 256), 256, 0, s>>>(a.g.n, field, chunks);
+  k_spread_clear<<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, field, chunks);
   LBM_LAUNCH_CHECK("ibm_spread_noalloc");
   if (pt->n_markers == 0) return LBM_OK;
   const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);

@@ -386,6 +386,74 @@ __device__ __forceinline__ void pull_general(const typename Storage<S>::T *__res
   PullGeneral<Q, S, WORK>::run(fa, g, x, y, z, face_rho, f);
 }
 
+constexpr int kMaxQ = 27;
+
+// Per-direction plane pointers of one step, computed on the host
+// (fill_step_planes), so that every population address in the kernels is
+// one 32 x 32 -> 64-bit multiply-add of the node index onto a parameter:
+//   src[i] + idx   row (x - ex, y - ey) of plane i of fa at the node's z: the
+//                  pull source of an interior row is src[i] + idx - ez;
+//   zlo[i] + idx   (ez > 0) source of a node at z = 0 under the bottom face
+//                  rule: PERIODICAL -> (i, x, y, nz - 1), else (rev i, x, y, 0);
+//   zhi[i] + idx   (ez < 0) source of a node at z = nz - 1 under the top face
+//                  rule: PERIODICAL -> (i, x, y, 0), else (rev i, x, y, nz - 1);
+//   dst[i] + idx   plane i of fb.
+struct StepPlanes {
+  const void *src[kMaxQ];
+  const void *zlo[kMaxQ];
+  const void *zhi[kMaxQ];
+  void *dst[kMaxQ];
+};
+
+// WALL_WITH_SPEED correction of the directions entering through z face FC
+// (4 = bottom, 5 = top) at a node of an interior row, applied after the
+// plain bounce-back pull: the same expression as pull_one's.
+template <int Q, int FC>
+__device__ __forceinline__ void zface_wws(const Geom &g, const float *__restrict__ face_rho,
+                                          int x, int y, int z, float f[Q]) {
+  using V = VSet<Q>;
+  const float rho_t = face_rho[plane_index(g, FC, x, y, z)];
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ez = V::ez(i);
+    if constexpr ((FC == 4 && ez > 0) || (FC == 5 && ez < 0)) {
+      const float eu = (float)V::ex(i) * g.uw[FC][0] + (float)V::ey(i) * g.uw[FC][1] +
+                       (float)ez * g.uw[FC][2];
+      f[i] = f[i] - 2.f * (rho_t * V::w(i)) * eu * g.inv_cs2;
+    }
+  });
+}
+
+// Pull of one node of an interior row (x, y not on a face): every source is
+// in row (x - ex, y - ey) except where the z face rule applies, which is
+// chosen by a select on the address (no branch, so all Q loads issue
+// together).  WORK: working values (d for the shifted storages) as the fused
+// step uses them; otherwise f, with the same values and corrections as
+// pull_general.
+template <int Q, int S, bool WORK>
+__device__ __forceinline__ void pull_row_node(const StepPlanes &p, const Geom &g,
+                                              const float *__restrict__ face_rho, unsigned idx,
+                                              int x, int y, int z, float f[Q]) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using V = VSet<Q>;
+  const bool bottom = z == 0, top = z == g.nz - 1;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ez = V::ez(i);
+    const T *ps = static_cast<const T *>(p.src[i]) + idx;
+    const T *src = ps;
+    if constexpr (ez > 0) src = bottom ? static_cast<const T *>(p.zlo[i]) + idx : ps - 1;
+    if constexpr (ez < 0) src = top ? static_cast<const T *>(p.zhi[i]) + idx : ps + 1;
+    if constexpr (WORK)
+      f[i] = St::work(src);
+    else
+      f[i] = St::load(src, V::w(i));
+  });
+  if (bottom && g.face[4] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 4>(g, face_rho, x, y, z, f);
+  if (top && g.face[5] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 5>(g, face_rho, x, y, z, f);
+}
+
 // Rolled value (periodic wrap on every axis, no face rule): what the
 // reference's f holds at a node before the face overrides run.  Used by the
 // NON_EQUILIBRIUM faces, which read plane 1 / plane X-2 right after the roll.

@@ -11,28 +11,10 @@
 namespace lbm {
 
 constexpr int kThreads = 256;
-constexpr int kMaxQ = 27;
 
 // ---------------------------------------------------------------------------
 // Fused step
 // ---------------------------------------------------------------------------
-// Per-direction plane pointers of one step, computed on the host
-// (fill_step_planes), so that every population address in the kernels is
-// one 32 x 32 -> 64-bit multiply-add of the node index onto a parameter:
-//   src[i] + idx   row (x - ex, y - ey) of plane i of fa at the node's z: the
-//                  pull source of an interior row is src[i] + idx - ez;
-//   zlo[i] + idx   (ez > 0) source of a node at z = 0 under the bottom face
-//                  rule: PERIODICAL -> (i, x, y, nz - 1), else (rev i, x, y, 0);
-//   zhi[i] + idx   (ez < 0) source of a node at z = nz - 1 under the top face
-//                  rule: PERIODICAL -> (i, x, y, 0), else (rev i, x, y, nz - 1);
-//   dst[i] + idx   plane i of fb.
-struct StepPlanes {
-  const void *src[kMaxQ];
-  const void *zlo[kMaxQ];
-  const void *zhi[kMaxQ];
-  void *dst[kMaxQ];
-};
-
 struct StepArgs {
   Geom g;
   NodeDecomp dec;
@@ -92,7 +74,10 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsig
     dev_moments<Q>(f, fox, foy, foz, face, rho, drho, ux, uy, uz);
   else
     moments<Q>(f, fox, foy, foz, face, rho, ux, uy, uz);
-  if (FORCE) {
+  // cul_equ2 and the second moment pass add nothing where this step's force
+  // is zero (everywhere outside the spread chunks when there is no uniform
+  // force), so such nodes skip them -- the same rule in every kernel.
+  if (FORCE && (fnx != 0.f || fny != 0.f || fnz != 0.f)) {
     add_force<Q>(f, a.g, ux, uy, uz, fnx, fny, fnz);
     if constexpr (DEV)
       dev_moments<Q>(f, fnx, fny, fnz, face, rho, drho, ux, uy, uz);
@@ -125,52 +110,6 @@ __device__ __forceinline__ void report_bad(unsigned *status, unsigned bad) {
   if (bad != 0 && status != nullptr) atomicOr(status, bad);
 }
 
-// WALL_WITH_SPEED correction of the directions entering through z face FC
-// (4 = bottom, 5 = top) at a node of an interior row, applied after the
-// plain bounce-back pull: the same expression as pull_one's.
-template <int Q, int FC>
-__device__ __forceinline__ void zface_wws(const Geom &g, const float *__restrict__ face_rho,
-                                          int x, int y, int z, float f[Q]) {
-  using V = VSet<Q>;
-  const float rho_t = face_rho[plane_index(g, FC, x, y, z)];
-  static_for<Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    constexpr int ez = V::ez(i);
-    if constexpr ((FC == 4 && ez > 0) || (FC == 5 && ez < 0)) {
-      const float eu = (float)V::ex(i) * g.uw[FC][0] + (float)V::ey(i) * g.uw[FC][1] +
-                       (float)ez * g.uw[FC][2];
-      f[i] = f[i] - 2.f * (rho_t * V::w(i)) * eu * g.inv_cs2;
-    }
-  });
-}
-
-// Pull of one node of an interior row (x, y not on a face): every source is
-// in row (x - ex, y - ey) except where the z face rule applies, which is
-// chosen by a select on the address (no branch, so all Q loads issue
-// together).
-template <int Q, int S>
-__device__ __forceinline__ void pull_row_node(const StepArgs &a, unsigned idx, int x, int y,
-                                              int z, float f[Q]) {
-  using St = Storage<S>;
-  using T = typename St::T;
-  using V = VSet<Q>;
-  const bool bottom = z == 0, top = z == a.g.nz - 1;
-  static_for<Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    constexpr int ez = V::ez(i);
-    const T *ps = static_cast<const T *>(a.p.src[i]) + idx;
-    if constexpr (ez == 0) {
-      f[i] = St::work(ps);
-    } else if constexpr (ez > 0) {
-      f[i] = St::work(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx : ps - 1);
-    } else {
-      f[i] = St::work(top ? static_cast<const T *>(a.p.zhi[i]) + idx : ps + 1);
-    }
-  });
-  if (bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, z, f);
-  if (top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, z, f);
-}
-
 // One node per thread, nodes in memory order so that each warp owns one
 // 32-node chunk.  Rows with interior (x, y) pull through pull_row_node;
 // rows on an x / y face take the general face rules.  FORCE adds cul_equ2
@@ -187,7 +126,7 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   float f[Q];
   if (row_in)
-    pull_row_node<Q, S>(a, idx, x, y, z, f);
+    pull_row_node<Q, S, true>(a.p, a.g, a.face_rho_in, idx, x, y, z, f);
   else
     pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, a.face_rho_in, f);
   unsigned bad = 0;
