@@ -74,10 +74,13 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsig
     dev_moments<Q>(f, fox, foy, foz, face, rho, drho, ux, uy, uz);
   else
     moments<Q>(f, fox, foy, foz, face, rho, ux, uy, uz);
-  // cul_equ2 and the second moment pass add nothing where this step's force
-  // is zero (everywhere outside the spread chunks when there is no uniform
-  // force), so such nodes skip them -- the same rule in every kernel.
-  if (FORCE && (fnx != 0.f || fny != 0.f || fnz != 0.f)) {
+  // Where both the previous and this step's force are zero (everywhere
+  // outside the spread chunks when there is no uniform force) cul_equ2 adds
+  // nothing and the second moment pass repeats the first, so such nodes skip
+  // them -- the same rule in every kernel.  (A zero new force alone is not
+  // enough: the second pass drops the previous force from u.)
+  if (FORCE && (fnx != 0.f || fny != 0.f || fnz != 0.f || fox != 0.f || foy != 0.f ||
+                foz != 0.f)) {
     add_force<Q>(f, a.g, ux, uy, uz, fnx, fny, fnz);
     if constexpr (DEV)
       dev_moments<Q>(f, fnx, fny, fnz, face, rho, drho, ux, uy, uz);
