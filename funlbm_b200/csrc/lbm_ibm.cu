@@ -304,16 +304,25 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
 // ---------------------------------------------------------------------------
 // Spreading (lbm/lbm3d.py:102-119)
 // ---------------------------------------------------------------------------
-// Clear the chunks written last time this buffer was used: one thread per
-// chunk (only a few chunks are flagged, so most threads read one byte).
+// Clear the chunks written last time this buffer was used.  Each lane reads
+// the flag of one chunk; the warp then clears its flagged chunks together
+// (3 floats per lane per chunk), so a mostly flagged small lattice costs no
+// more than a sparse large one.
 __global__ void k_spread_clear(long long n, float *field, uint8_t *chunks) {
   const long long chunk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nchunks = (n + 31) >> 5;
-  if (chunk >= nchunks || chunks[chunk] == 0) return;
-  const long long first = chunk * 32;
-  const long long last = first + 32 < n ? first + 32 : n;
-  for (long long k = 3 * first; k < 3 * last; ++k) field[k] = 0.f;
-  chunks[chunk] = 0;
+  const int lane = threadIdx.x & 31;
+  const bool mine = chunk < nchunks && chunks[chunk] != 0;
+  unsigned todo = __ballot_sync(0xffffffffu, mine);
+  const long long base = chunk - lane;   // first chunk of this warp
+  while (todo != 0) {
+    const int j = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const long long first = (base + j) * 32;
+    const long long count = 3 * ((first + 32 < n ? first + 32 : n) - first);
+    for (long long k = lane; k < count; k += 32) field[3 * first + k] = 0.f;
+  }
+  if (mine) chunks[chunk] = 0;
 }
 
 struct SpreadArgs {

@@ -53,18 +53,36 @@ __device__ __forceinline__ unsigned bad_bits(float rho, float ux, float uy, floa
 // densities, observation, and (when fb is set) the next step's collision, in
 // place in f.  DEV: f holds deviations d = f - w (shifted storage), handled
 // by dev_moments / collide_dev.
+// Whether the previous / this step's force field applies in the 32-node
+// chunk of node idx.  A thread's nodes always share one chunk, so the kernels
+// read the flags once, before their population loads.
+struct ChunkForce {
+  bool old_here, new_here;
+};
+
+template <bool FORCE>
+__device__ __forceinline__ ChunkForce chunk_force(const StepArgs &a, unsigned idx) {
+  ChunkForce c{false, false};
+  if constexpr (FORCE) {
+    c.old_here = a.fol_old != nullptr && (a.ch_old == nullptr || a.ch_old[idx >> 5]);
+    c.new_here = a.fol_new != nullptr && (a.ch_new == nullptr || a.ch_new[idx >> 5]);
+  }
+  return c;
+}
+
 template <int Q, bool FORCE, bool DEV>
 __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsigned idx, int x,
-                                            int y, int z, bool face, unsigned &bad) {
+                                            int y, int z, bool face, ChunkForce cf,
+                                            unsigned &bad) {
   using V = VSet<Q>;
   float fox = a.go[0], foy = a.go[1], foz = a.go[2];
   float fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
-  if (a.fol_old != nullptr && (a.ch_old == nullptr || a.ch_old[idx >> 5])) {
+  if (cf.old_here) {
     fox += a.fol_old[3ull * idx];
     foy += a.fol_old[3ull * idx + 1];
     foz += a.fol_old[3ull * idx + 2];
   }
-  if (a.fol_new != nullptr && (a.ch_new == nullptr || a.ch_new[idx >> 5])) {
+  if (cf.new_here) {
     fnx += a.fol_new[3ull * idx];
     fny += a.fol_new[3ull * idx + 1];
     fnz += a.fol_new[3ull * idx + 2];
@@ -125,6 +143,7 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   using T = typename St::T;
   if (idx >= (unsigned)a.g.n) return;
   int x, y, z;
+  const ChunkForce cf = chunk_force<FORCE>(a, idx);
   a.dec(idx, x, y, z);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   float f[Q];
@@ -133,7 +152,8 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   else
     pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, a.face_rho_in, f);
   unsigned bad = 0;
-  finish_node<Q, FORCE, St::kDev>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1, bad);
+  finish_node<Q, FORCE, St::kDev>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1, cf,
+                                  bad);
   report_bad(a.status, bad);
   if (a.fb != nullptr) {
     static_for<Q>([&](auto ic) {
@@ -175,6 +195,7 @@ __device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned
   const unsigned idx0 = t * NZ;
   if (idx0 >= (unsigned)a.g.n) return;
   int x, y, z0;
+  const ChunkForce cf = chunk_force<FORCE>(a, idx0);
   a.dec(idx0, x, y, z0);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
@@ -224,9 +245,9 @@ __device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned
       pull_general<Q, S, true>(fa, a.g, x, y, za + 1, a.face_rho_in, f1);
     }
     finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
-                                !row_in || za == 0 || za == a.g.nz - 1, bad);
+                                !row_in || za == 0 || za == a.g.nz - 1, cf, bad);
     finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
-                                !row_in || za + 1 == 0 || za + 1 == a.g.nz - 1, bad);
+                                !row_in || za + 1 == 0 || za + 1 == a.g.nz - 1, cf, bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -251,6 +272,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   const unsigned idx0 = t * NZ;
   if (idx0 >= (unsigned)a.g.n) return;
   int x, y, z0;
+  const ChunkForce cf = chunk_force<FORCE>(a, idx0);
   a.dec(idx0, x, y, z0);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   float f[NZ][Q];
@@ -303,7 +325,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   for (int k = 0; k < NZ; ++k) {
     const int z = z0 + k;
     finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z,
-                                    !row_in || z == 0 || z == a.g.nz - 1, bad);
+                                    !row_in || z == 0 || z == a.g.nz - 1, cf, bad);
   }
   report_bad(a.status, bad);
   if (a.fb == nullptr) return;
@@ -511,6 +533,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
       row_xy(r, x, y);
       const int z = 2 * zp;
       const unsigned idx = (unsigned)(r * nz + z);
+      const ChunkForce cf = chunk_force<FORCE>(a, idx);
       float f0[Q], f1[Q];
       const bool row_in = interior(x, y);
       if (row_in) {
@@ -542,8 +565,9 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
         pull_general<Q, S, true>(fa, a.g, x, y, z + 1, a.face_rho_in, f1);
       }
       unsigned bad = 0;
-      finish_node<Q, FORCE, St::kDev>(a, f0, idx, x, y, z, !row_in || z == 0, bad);
-      finish_node<Q, FORCE, St::kDev>(a, f1, idx + 1, x, y, z + 1, !row_in || z + 1 == nz - 1, bad);
+      finish_node<Q, FORCE, St::kDev>(a, f0, idx, x, y, z, !row_in || z == 0, cf, bad);
+      finish_node<Q, FORCE, St::kDev>(a, f1, idx + 1, x, y, z + 1, !row_in || z + 1 == nz - 1, cf,
+                                      bad);
       report_bad(a.status, bad);
       if (a.fb != nullptr) {
         static_for<Q>([&](auto ic) {
