@@ -337,3 +337,61 @@ def test_launch_shapes_agree_bitwise(q, storage):
     ref = results[(1, 256)]
     for k, v in results.items():
         assert np.array_equal(v, ref), (k, np.abs(v - ref).max())
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("storage", ["fp32", "fp16s"])
+def test_chunked_force_fields_agree_bitwise(q, storage):
+    """Force fields present only in some 32-node chunks, as spreading leaves
+    them: chunks with a previous and a new field, with only the previous one
+    (the second moment pass must drop it from u), with only the new one, and
+    none.  Every launch shape -- the forced kernels run the unforced code for
+    chunks without any force -- gives the same bits."""
+    from funlbm_b200.lattice import Lattice, make_force, tau_float32
+    from funlbm_b200.tune import CANDIDATES, shape_ok
+
+    shape = (10, 9, 64)
+    n = shape[0] * shape[1] * shape[2]
+    nch = (n + 31) // 32
+    rng = np.random.default_rng(7 + q)
+    kind = rng.integers(0, 4, nch)            # 0 none, 1 old only, 2 new only, 3 both
+    kind[:4] = [0, 1, 2, 3]
+    ch_old = torch.tensor(((kind == 1) | (kind == 3)).astype(np.uint8), device="cuda")
+    ch_new = torch.tensor(((kind == 2) | (kind == 3)).astype(np.uint8), device="cuda")
+    node_kind = np.repeat(kind, 32)[:n]
+    f_old = 1e-4 * rng.standard_normal((n, 3)).astype(np.float32)
+    f_new = 1e-4 * rng.standard_normal((n, 3)).astype(np.float32)
+    f_old[~np.isin(node_kind, (1, 3))] = 0
+    f_new[~np.isin(node_kind, (2, 3))] = 0
+    F_old = torch.tensor(f_old.reshape(-1), device="cuda")
+    F_new = torch.tensor(f_new.reshape(-1), device="cuda")
+    force = make_force((0, 0, 0), (0, 0, 0), F_old, F_new, ch_old, ch_new)
+    codes = [1200, 1200, 11000, 11000, 1200, 11000]
+    f0 = smooth_f0(q, shape, 0.04, q + 3)
+    f0_soa = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda")
+    bits = 32 if storage == "fp32" else 16
+    results = {}
+    for nodes, threads in CANDIDATES[bits]:
+        if not shape_ok(nodes, shape[2], bits):
+            continue
+        lat = Lattice(q, shape, codes, tau_float32(0.07), storage=storage, device="cuda")
+        lat.set_launch_shape(nodes, threads)
+        lat.init(f0_soa)
+        for _ in range(3):
+            lat.step(force)
+        assert lat.read_status() == 0
+        f = torch.empty(q * lat.n, device="cuda")
+        lat.observe(force, f=f)
+        results[(nodes, threads)] = to_np(f)
+    ref = results[(1, 256)]
+    assert len(results) >= 4
+    for k, v in results.items():
+        assert np.array_equal(v, ref), (k, np.abs(v - ref).max())
+    # and the fields did act: without them the state differs
+    lat = Lattice(q, shape, codes, tau_float32(0.07), storage=storage, device="cuda")
+    lat.init(f0_soa)
+    for _ in range(3):
+        lat.step(None)
+    f = torch.empty(q * lat.n, device="cuda")
+    lat.observe(None, f=f)
+    assert not np.array_equal(to_np(f), ref)
