@@ -725,8 +725,9 @@ struct StepLauncher {
       // measured on B200 at 512^3: 2 nodes per thread with 128-thread blocks
       // is the fastest shape for every velocity set and storage, except
       // D3Q19 in 16-bit storage, where 4 nodes per thread (register-capped)
-      // are (see funlbm_b200.tune)
-      const int want = (bits == 16 && Q == 19) ? 4 : 2;
+      // are -- unforced only: the forced 4-node kernel spills (see
+      // funlbm_b200.tune)
+      const int want = (bits == 16 && Q == 19 && !force) ? 4 : 2;
       nodes = step_shape_ok(want, a.g.nz, bits) ? want : step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
       threads = threads ? threads : 128;
     }

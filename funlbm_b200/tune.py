@@ -90,7 +90,8 @@ def class_key(lat, forced):
 def tune_class(lat, forced=False, iters=6, warmup=2):
     """Launch shape for ``lat`` from its class -- velocity set, storage,
     which vector widths its rows allow, forced or not -- tuned once per class
-    on a ~96^3 proxy with the lattice's faces and cached.  Meant for servers
+    on a ~96^3 proxy with the lattice's faces (forced: force fields in 5 % of
+    the 32-node chunks, as spreading leaves them) and cached.  Meant for servers
     that see many lattice sizes: one short tuning per class instead of one per
     (ny, nz).  Returns the choice."""
     from .lattice import Lattice, make_force
@@ -103,7 +104,18 @@ def tune_class(lat, forced=False, iters=6, warmup=2):
         proxy = Lattice(lat.q, (n, n, nz), lat.faces, lat.tau, storage=lat.storage,
                         face_uw=lat.face_uw, re_mu=lat.re_mu, device=lat.device)
         proxy.init(None)
-        force = make_force((0, 0, 0), (1e-6, 0, 0)) if forced else None
+        force, keep = None, None
+        if forced:
+            # spread forces as IBM leaves them: fields in a few percent of the
+            # 32-node chunks, none elsewhere (most threads run force-free)
+            pn = proxy.n
+            nch = (pn + 31) // 32
+            g = torch.Generator(device="cpu").manual_seed(0)
+            flags = (torch.rand(nch, generator=g) < 0.05).to(torch.uint8)
+            field = 1e-5 * torch.randn(pn, 3, generator=g)
+            field[(flags.repeat_interleave(32)[:pn] == 0)] = 0
+            keep = [field.reshape(-1).to(lat.device), flags.to(lat.device)]
+            force = make_force((0, 0, 0), (0, 0, 0), keep[0], keep[0], keep[1], keep[1])
         bits = 32 if lat.storage == "fp32" else 16
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
