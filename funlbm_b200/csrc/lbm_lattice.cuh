@@ -113,9 +113,6 @@ struct VSet<27> {
 template <int S>
 struct Storage;
 
-// from_bits / to_bits convert one stored element held in the low bits of a
-// 32-bit word (used by the vectorised loads and stores).
-//
 // The fused step works on the stored quantity itself (its "working value"):
 // f for FP32, the deviation d = f - w_i for the shifted forms (kDev), whose
 // moments and collision are restated for d (dev_moments / collide_dev), so
@@ -132,8 +129,6 @@ struct Storage<LBM_STORAGE_FP32> {
   __device__ __forceinline__ static void put(T *p, float v) { *p = v; }
   __device__ __forceinline__ static float load(const T *p, float) { return __ldg(p); }
   __device__ __forceinline__ static void store(T *p, float v, float) { *p = v; }
-  __device__ __forceinline__ static float from_bits(unsigned b, float) { return __uint_as_float(b); }
-  __device__ __forceinline__ static unsigned to_bits(float v, float) { return __float_as_uint(v); }
 };
 template <>
 struct Storage<LBM_STORAGE_FP16S> {
@@ -149,12 +144,6 @@ struct Storage<LBM_STORAGE_FP16S> {
   }
   __device__ __forceinline__ static void store(T *p, float v, float w) {
     *p = __float2half_rn(v - w);
-  }
-  __device__ __forceinline__ static float from_bits(unsigned b, float w) {
-    return w + __half2float(__ushort_as_half((unsigned short)(b & 0xffffu)));
-  }
-  __device__ __forceinline__ static unsigned to_bits(float v, float w) {
-    return (unsigned)__half_as_ushort(__float2half_rn(v - w));
   }
 };
 template <>
@@ -172,44 +161,7 @@ struct Storage<LBM_STORAGE_BF16S> {
   __device__ __forceinline__ static void store(T *p, float v, float w) {
     *p = __float2bfloat16_rn(v - w);
   }
-  __device__ __forceinline__ static float from_bits(unsigned b, float w) {
-    return w + __bfloat162float(__ushort_as_bfloat16((unsigned short)(b & 0xffffu)));
-  }
-  __device__ __forceinline__ static unsigned to_bits(float v, float w) {
-    return (unsigned)__bfloat16_as_ushort(__float2bfloat16_rn(v - w));
-  }
 };
-
-// Two consecutive 16-bit elements in one 32-bit word (low half first).
-template <int S>
-__device__ __forceinline__ float2 unpack2(unsigned word, float w);
-template <>
-__device__ __forceinline__ float2 unpack2<LBM_STORAGE_FP16S>(unsigned word, float w) {
-  __half2 h;
-  memcpy(&h, &word, 4);
-  const float2 v = __half22float2(h);
-  return make_float2(v.x + w, v.y + w);
-}
-template <>
-__device__ __forceinline__ float2 unpack2<LBM_STORAGE_BF16S>(unsigned word, float w) {
-  return make_float2(__uint_as_float(word << 16) + w, __uint_as_float(word & 0xffff0000u) + w);
-}
-template <int S>
-__device__ __forceinline__ unsigned pack2(float a, float b, float w);
-template <>
-__device__ __forceinline__ unsigned pack2<LBM_STORAGE_FP16S>(float a, float b, float w) {
-  const __half2 h = __floats2half2_rn(a - w, b - w);
-  unsigned word;
-  memcpy(&word, &h, 4);
-  return word;
-}
-template <>
-__device__ __forceinline__ unsigned pack2<LBM_STORAGE_BF16S>(float a, float b, float w) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(a - w, b - w);
-  unsigned word;
-  memcpy(&word, &h, 4);
-  return word;
-}
 
 // Two consecutive stored elements <-> two working values (low element first).
 template <int S>
