@@ -192,8 +192,34 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 // NZ - |ez| of the NZ values, one scalar load the remaining one -- from the
 // neighbouring vector, or at z = 0 / z = nz - 1 from the bottom / top face
 // rule, picked by an address select so that all loads issue together.
-// Rows on an x / y face take the per-node face rules.
+// Rows on an x / y face take the per-node face rules (face_row_nodes).
 // ---------------------------------------------------------------------------
+// Nodes of a row on an x / y face (under 1 % of a large lattice): one at a
+// time through the general face rules, in a loop that is not unrolled, so
+// the vector kernels carry one copy of this code instead of NZ and their hot
+// path stays compact in the instruction cache.  Same per-node arithmetic.
+template <int Q, int S, bool FORCE>
+__device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, int count, int x,
+                                               int y, int z0, ChunkForce cf) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  const T *fa = static_cast<const T *>(a.fa);
+  unsigned bad = 0;
+#pragma unroll 1
+  for (int k = 0; k < count; ++k) {
+    float f[Q];
+    pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, a.face_rho_in, f);
+    finish_node<Q, FORCE, St::kDev>(a, f, idx0 + k, x, y, z0 + k, true, cf, bad);
+    if (a.fb != nullptr) {
+      static_for<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        St::put(static_cast<T *>(a.p.dst[i]) + idx0 + k, f[i]);
+      });
+    }
+  }
+  report_bad(a.status, bad);
+}
+
 // 16-bit storage: the vectors stay packed in registers and are unpacked one
 // node pair at a time, right before that pair is finished and stored (one
 // 32-bit word per direction), so a thread holds 2 x Q floats instead of
@@ -214,27 +240,29 @@ __device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned
   const ChunkForce cf = chunk_force<FORCE>(a, idx0);
   a.dec(idx0, x, y, z0);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
+  if (!row_in) {
+    face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0, cf);
+    return;
+  }
   const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
   Words<kWords> raw[Q];
   T extra[Q];
-  if (row_in) {
-    static_for<Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      constexpr int ez = V::ez(i);
-      const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
-      raw[i] = ld_words<kWords>(ps);
-      if constexpr (ez > 0)
-        extra[i] = St::raw(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx0 : ps - 1);
-      if constexpr (ez < 0)
-        extra[i] = St::raw(top ? static_cast<const T *>(a.p.zhi[i]) + (idx0 + NZ - 1) : ps + NZ);
-    });
-  }
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ez = V::ez(i);
+    const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
+    raw[i] = ld_words<kWords>(ps);
+    if constexpr (ez > 0)
+      extra[i] = St::raw(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx0 : ps - 1);
+    if constexpr (ez < 0)
+      extra[i] = St::raw(top ? static_cast<const T *>(a.p.zhi[i]) + (idx0 + NZ - 1) : ps + NZ);
+  });
   unsigned bad = 0;
 #pragma unroll
   for (int pr = 0; pr < kWords; ++pr) {
     float f0[Q], f1[Q];
     const int za = z0 + 2 * pr;
-    if (row_in) {
+    {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         constexpr int ez = V::ez(i);
@@ -255,15 +283,11 @@ __device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned
         zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f0);
       if (pr == kWords - 1 && top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
         zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, a.g.nz - 1, f1);
-    } else {
-      const T *fa = static_cast<const T *>(a.fa);
-      pull_general<Q, S, true>(fa, a.g, x, y, za, a.face_rho_in, f0);
-      pull_general<Q, S, true>(fa, a.g, x, y, za + 1, a.face_rho_in, f1);
     }
-    finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
-                                !row_in || za == 0 || za == a.g.nz - 1, cf, bad);
-    finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
-                                !row_in || za + 1 == 0 || za + 1 == a.g.nz - 1, cf, bad);
+    finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za, za == 0 || za == a.g.nz - 1, cf,
+                                bad);
+    finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1, za + 1 == a.g.nz - 1, cf,
+                                bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -297,8 +321,12 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   const ChunkForce cf = chunk_force<FORCE>(a, idx0);
   a.dec(idx0, x, y, z0);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
+  if (!row_in) {
+    face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0, cf);
+    return;
+  }
   float f[NZ][Q];
-  if (row_in) {
+  {
     const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
@@ -335,19 +363,14 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
       zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f[0]);
     if (top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
       zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, a.g.nz - 1, f[NZ - 1]);
-  } else {
-    const T *fa = static_cast<const T *>(a.fa);
-#pragma unroll
-    for (int k = 0; k < NZ; ++k)
-      pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, a.face_rho_in, f[k]);
   }
 
   unsigned bad = 0;
 #pragma unroll
   for (int k = 0; k < NZ; ++k) {
     const int z = z0 + k;
-    finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z,
-                                    !row_in || z == 0 || z == a.g.nz - 1, cf, bad);
+    finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z, z == 0 || z == a.g.nz - 1, cf,
+                                    bad);
   }
   report_bad(a.status, bad);
   if (a.fb == nullptr) return;
@@ -367,13 +390,14 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
 
 // Register cap of the vectorised step for 16-bit storage, as resident blocks
 // per SM asked of the compiler (0 = no cap).  A 16-bit population costs a
-// whole float register once unpacked, so without a cap the 4-node 16-bit
-// kernels of D3Q15 / D3Q19 hold too few bytes in flight per SM to cover HBM
-// latency; the cap (measured on B200 at 512^3) trades a few spilled words
-// for a third more resident warps.  FP32 runs uncapped.
+// whole float register once unpacked, so the 16-bit kernels hold too few
+// bytes in flight per SM to cover HBM latency unless enough warps are
+// resident; these caps (measured on B200 at 512^3, none of them spills)
+// trade register slack for resident warps.  FP32 runs uncapped.
 template <int Q, int S, int NZ>
 constexpr int vec_reg_cap() {
   if (Storage<S>::kBits == 32) return 0;
+  if (NZ == 2) return Q == 19 ? 72 : Q == 27 ? 96 : 0;
   if (NZ == 4) return Q == 15 || Q == 19 ? 128 : 0;
   return 0;
 }
