@@ -420,21 +420,23 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
 // per SM asked of the compiler (0 = no cap).  A 16-bit population costs a
 // whole float register once unpacked, so the 16-bit kernels hold too few
 // bytes in flight per SM to cover HBM latency unless enough warps are
-// resident; these caps (measured on B200 at 512^3, none of them spills)
-// trade register slack for resident warps.  FP32 runs uncapped.
-template <int Q, int S, int NZ>
+// resident; these caps (measured on B200 at 512^3 and on lattices with
+// particles; none of them spills) trade register slack for resident warps.
+// FP32 runs uncapped.
+template <int Q, int S, int NZ, bool FORCE>
 constexpr int vec_reg_cap() {
   if (Storage<S>::kBits == 32) return 0;
+  if (NZ == 2 && FORCE) return Q == 19 ? 72 : Q == 27 ? 96 : 0;
   if (NZ == 4) return Q == 15 || Q == 19 ? 128 : 0;
   return 0;
 }
-template <int Q, int S, int NZ, int TB>
+template <int Q, int S, int NZ, int TB, bool FORCE>
 constexpr int vec_min_blocks() {
-  return vec_reg_cap<Q, S, NZ>() == 0 ? 0 : 65536 / (vec_reg_cap<Q, S, NZ>() * TB);
+  return vec_reg_cap<Q, S, NZ, FORCE>() == 0 ? 0 : 65536 / (vec_reg_cap<Q, S, NZ, FORCE>() * TB);
 }
 
 template <int Q, int S, bool FORCE, int NZ, int TB>
-__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB>())) k_step_vec(const StepArgs a) {
+__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>())) k_step_vec(const StepArgs a) {
   step_vec_body<Q, S, FORCE, NZ>(a, blockIdx.x * TB + threadIdx.x);
 }
 
@@ -450,7 +452,7 @@ __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB>())) k_step_v
 constexpr int kBatchTiles = 4;   // tiles of TB threads per block (amortises the lookup)
 
 template <int Q, int S, bool FORCE, int NZ, int TB>
-__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB>()))
+__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>()))
     k_step_batch(const StepArgs *__restrict__ entries, const unsigned *__restrict__ block_begin,
                  int count) {
   __shared__ __align__(16) StepArgs sa;
