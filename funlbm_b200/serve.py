@@ -205,6 +205,25 @@ class LBMServer:
         self.stats["max_used_bytes"] = max(self.stats["max_used_bytes"], self.used)
         return admitted
 
+    def prepare(self, requests):
+        """Tune the launch-shape classes these requests will need, ahead of
+        serving them (a running server keeps the choices cached, so only the
+        first requests of a new class would otherwise pay for the tuning)."""
+        if not self.tune:
+            return
+        from .tune import tune_class_of
+
+        with torch.cuda.stream(self._init_stream):
+            for r in requests:
+                flow = r.config.get("flow") or {}
+                q = int(str(flow.get("param_type") or "D3Q19")[3:])
+                storage = ((flow.get("precision") or {}).get("storage")) or "fp32"
+                nz = _shape_of(r.config)[2]
+                forced = bool(r.config.get("particles")) or any(
+                    float(v) != 0.0 for v in (flow.get("body_force") or ()))
+                tune_class_of(q, storage, nz, forced, device=self.device)
+        torch.cuda.synchronize(self.device)
+
     def _tune(self, lbm):
         """Launch shape of this request's step kernel from the autotuner (per
         class of lattice, cached), before any graph captures it."""

@@ -81,61 +81,71 @@ _CLASS_CACHE = {}
 CLASS_PROXY_NODES = 96          # proxy lattice of a class: about 96^3 nodes
 
 
-def class_key(lat, forced):
-    nz = lat.shape[2]
-    return (lat.q, lat.storage, nz % 2 == 0 and nz >= 4, nz % 4 == 0 and nz >= 8,
+def class_key_of(q, storage, nz, forced):
+    return (int(q), storage, nz % 2 == 0 and nz >= 4, nz % 4 == 0 and nz >= 8,
             nz % 8 == 0 and nz >= 16, bool(forced))
 
 
-def tune_class(lat, forced=False, iters=6, warmup=2):
-    """Launch shape for ``lat`` from its class -- velocity set, storage,
-    which vector widths its rows allow, forced or not -- tuned once per class
-    on a ~96^3 proxy with the lattice's faces (forced: force fields in 5 % of
-    the 32-node chunks, as spreading leaves them) and cached.  Meant for servers
-    that see many lattice sizes: one short tuning per class instead of one per
-    (ny, nz).  Returns the choice."""
-    from .lattice import Lattice, make_force
+def class_key(lat, forced):
+    return class_key_of(lat.q, lat.storage, lat.shape[2], forced)
 
-    key = class_key(lat, forced)
-    if key not in _CLASS_CACHE:
-        _, even, by4, by8, _ = key[1:]
-        nz = 96 if by8 else 100 if by4 else 98 if even else 97
-        n = CLASS_PROXY_NODES
-        proxy = Lattice(lat.q, (n, n, nz), lat.faces, lat.tau, storage=lat.storage,
-                        face_uw=lat.face_uw, re_mu=lat.re_mu, device=lat.device)
-        proxy.init(None)
-        force, keep = None, None
-        if forced:
-            # spread forces as IBM leaves them: fields in a few percent of the
-            # 32-node chunks, none elsewhere (most threads run force-free)
-            pn = proxy.n
-            nch = (pn + 31) // 32
-            g = torch.Generator(device="cpu").manual_seed(0)
-            flags = (torch.rand(nch, generator=g) < 0.05).to(torch.uint8)
-            field = 1e-5 * torch.randn(pn, 3, generator=g)
-            field[(flags.repeat_interleave(32)[:pn] == 0)] = 0
-            keep = [field.reshape(-1).to(lat.device), flags.to(lat.device)]
-            force = make_force((0, 0, 0), (0, 0, 0), keep[0], keep[0], keep[1], keep[1])
-        bits = 32 if lat.storage == "fp32" else 16
-        start = torch.cuda.Event(enable_timing=True)
-        stop = torch.cuda.Event(enable_timing=True)
-        timings = {}
-        for nodes, threads in CANDIDATES[bits]:
-            if nodes == ROWS or not shape_ok(nodes, nz, bits):
-                continue
-            proxy.set_launch_shape(nodes, threads)
-            for _ in range(warmup):
-                proxy.step(force)
-            start.record()
-            for _ in range(iters):
-                proxy.step(force)
-            stop.record()
-            stop.synchronize()
-            timings[(nodes, threads)] = start.elapsed_time(stop) / iters
-        proxy.release()
-        del proxy
-        _CLASS_CACHE[key] = min(timings, key=timings.get)
-    choice = _CLASS_CACHE[key]
+
+def tune_class_of(q, storage, nz, forced, device="cuda", iters=6, warmup=2):
+    """Launch shape of the class (velocity set, storage, which vector widths
+    rows of nz nodes allow, forced or not), tuned once per class on a ~96^3
+    periodic proxy (forced: force fields in 5 % of the 32-node chunks, as
+    spreading leaves them) and cached.  Meant for servers that see many
+    lattice sizes: one short tuning per class instead of one per (ny, nz).
+    Returns (nodes, threads)."""
+    from .lattice import Lattice, make_force, tau_float32
+
+    key = class_key_of(q, storage, nz, forced)
+    if key in _CLASS_CACHE:
+        return _CLASS_CACHE[key]
+    _, _, even, by4, by8, _ = key
+    pnz = 96 if by8 else 100 if by4 else 98 if even else 97
+    n = CLASS_PROXY_NODES
+    proxy = Lattice(int(q), (n, n, pnz), [11000] * 6, tau_float32(0.05), storage=storage,
+                    device=device)
+    proxy.init(None)
+    force, keep = None, None
+    if forced:
+        # spread forces as IBM leaves them: fields in a few percent of the
+        # 32-node chunks, none elsewhere (most threads run force-free)
+        pn = proxy.n
+        nch = (pn + 31) // 32
+        dev = proxy.device
+        g = torch.Generator(device="cpu").manual_seed(0)
+        flags = (torch.rand(nch, generator=g) < 0.05).to(torch.uint8).to(dev)
+        field = 1e-5 * torch.randn(pn, 3, device=dev)
+        field *= flags.repeat_interleave(32)[:pn, None].to(field.dtype)
+        keep = [field.reshape(-1), flags]
+        force = make_force((0, 0, 0), (0, 0, 0), keep[0], keep[0], keep[1], keep[1])
+    bits = 32 if storage == "fp32" else 16
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    timings = {}
+    for nodes, threads in CANDIDATES[bits]:
+        if nodes == ROWS or not shape_ok(nodes, pnz, bits):
+            continue
+        proxy.set_launch_shape(nodes, threads)
+        for _ in range(warmup):
+            proxy.step(force)
+        start.record()
+        for _ in range(iters):
+            proxy.step(force)
+        stop.record()
+        stop.synchronize()
+        timings[(nodes, threads)] = start.elapsed_time(stop) / iters
+    proxy.release()
+    del proxy
+    _CLASS_CACHE[key] = min(timings, key=timings.get)
+    return _CLASS_CACHE[key]
+
+
+def tune_class(lat, forced=False):
+    """Set ``lat``'s launch shape to its class's tuned choice (tune_class_of)."""
+    choice = tune_class_of(lat.q, lat.storage, lat.shape[2], forced, device=lat.device)
     lat.set_launch_shape(*choice)
     return choice
 

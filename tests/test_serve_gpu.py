@@ -68,6 +68,8 @@ def test_results_same_alone_and_in_mix(mode):
 
     reqs = [Request(cfg, steps) for cfg, steps in CASES]
     server = LBMServer(budget_bytes=8e9, chunk=8, mode=mode, streams=4)
+    if mode == "streams":
+        server.prepare(reqs[:2])      # some classes tuned ahead, the rest at admission
     done = server.run(reqs, realtime=False)
     assert len(done) == len(CASES)
     assert server.stats["graph_replays"] > 0 and server.stats["max_active"] == len(CASES)
