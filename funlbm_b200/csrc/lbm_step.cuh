@@ -70,16 +70,6 @@ __device__ __forceinline__ ChunkForce chunk_force(const StepArgs &a, unsigned id
   return c;
 }
 
-// No force at all for this thread's nodes: no field in its chunk, now or in
-// the previous step, and no uniform force.  A forced kernel then runs the
-// unforced body for the thread, which gives the same bits (the forcing pass
-// would be skipped node by node anyway) with the unforced kernel's smaller
-// register footprint.
-__device__ __forceinline__ bool force_free(const StepArgs &a, ChunkForce cf) {
-  return !cf.old_here && !cf.new_here && a.go[0] == 0.f && a.go[1] == 0.f && a.go[2] == 0.f &&
-         a.gn[0] == 0.f && a.gn[1] == 0.f && a.gn[2] == 0.f;
-}
-
 template <int Q, bool FORCE, bool DEV>
 __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsigned idx, int x,
                                             int y, int z, bool face, ChunkForce cf,
@@ -154,12 +144,6 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   if (idx >= (unsigned)a.g.n) return;
   int x, y, z;
   const ChunkForce cf = chunk_force<FORCE>(a, idx);
-  if constexpr (FORCE) {
-    if (force_free(a, cf)) {
-      step_scalar_body<Q, S, false>(a, idx);
-      return;
-    }
-  }
   a.dec(idx, x, y, z);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   float f[Q];
@@ -323,12 +307,6 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
-  if constexpr (FORCE) {
-    if (t * NZ < (unsigned)a.g.n && force_free(a, chunk_force<true>(a, t * NZ))) {
-      step_vec_body<Q, S, false, NZ, COMPACT>(a, t);
-      return;
-    }
-  }
   if constexpr (St::kBits == 16 && NZ == 2) {
     step_vec_pairs<Q, S, FORCE, NZ, COMPACT>(a, t);
     return;

@@ -345,8 +345,8 @@ def test_chunked_force_fields_agree_bitwise(q, storage):
     """Force fields present only in some 32-node chunks, as spreading leaves
     them: chunks with a previous and a new field, with only the previous one
     (the second moment pass must drop it from u), with only the new one, and
-    none.  Every launch shape -- the forced kernels run the unforced code for
-    chunks without any force -- gives the same bits."""
+    none.  Every launch shape -- the forced kernels skip the forcing pass at
+    nodes without any force -- gives the same bits."""
     from funlbm_b200.lattice import Lattice, make_force, tau_float32
     from funlbm_b200.tune import CANDIDATES, shape_ok
 
