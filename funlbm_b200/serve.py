@@ -158,8 +158,6 @@ class LBMServer:
         self.queue.sort(key=lambda r: r.arrival)
 
     def _admit(self, now):
-        from .lbm import LBMD3, Config
-
         admitted = False
         i = 0
         while i < len(self.queue) and len(self.active) < self.max_slots:
@@ -175,35 +173,51 @@ class LBMServer:
             cfg.setdefault("log_per_steps", 10 ** 9)
             cfg.setdefault("file", {"per_steps": 10 ** 9})
             cfg["device"] = str(self.device)
-            if self.mode == "streams":
-                init = self._init_stream
-                with torch.cuda.stream(init):
-                    lbm = LBMD3(config=Config().from_json(cfg))
-                    lbm.init()
-                    slot = _Slot(req, lbm, nbytes)
-                    # the first step enters the fused representation (allocates)
-                    lbm.run_step(step=lbm.step)
-                    lbm.step += 1
-                    slot.remaining -= 1
-                    self.stats["eager_steps"] += 1
-                    self._tune(lbm)
-                    ready = torch.cuda.Event()
-                    ready.record(init)
-                slot.stream = self._pick_stream()
-                slot.stream.wait_event(ready)
-                self._top_up(slot)
-            else:
-                lbm = LBMD3(config=Config().from_json(cfg))
-                lbm.init()
-                slot = _Slot(req, lbm, nbytes)
+            try:
+                slot = self._start(req, cfg, nbytes)
+            except (ValueError, NotImplementedError, TypeError, KeyError) as e:
+                # the solver refused this config (the reference's error types):
+                # report it on the request and keep serving the others
+                req.result = {"error": "%s: %s" % (type(e).__name__, e)}
+                req.admitted_at = req.finished_at = now if now != float("inf") else 0.0
+                self.done.append(req)
+                self.stats["rejected"] = self.stats.get("rejected", 0) + 1
+                continue
             req.admitted_at = now
-            req.nodes = lbm.flow.n
+            req.nodes = slot.lbm.flow.n
             self.active.append(slot)
             self.used += nbytes
             admitted = True
         self.stats["max_active"] = max(self.stats["max_active"], len(self.active))
         self.stats["max_used_bytes"] = max(self.stats["max_used_bytes"], self.used)
         return admitted
+
+    def _start(self, req, cfg, nbytes):
+        """Build one admitted request on the device (and, in streams mode, run
+        its first step and enqueue its first chunks)."""
+        from .lbm import LBMD3, Config
+
+        if self.mode != "streams":
+            lbm = LBMD3(config=Config().from_json(cfg))
+            lbm.init()
+            return _Slot(req, lbm, nbytes)
+        init = self._init_stream
+        with torch.cuda.stream(init):
+            lbm = LBMD3(config=Config().from_json(cfg))
+            lbm.init()
+            slot = _Slot(req, lbm, nbytes)
+            # the first step enters the fused representation (allocates)
+            lbm.run_step(step=lbm.step)
+            lbm.step += 1
+            slot.remaining -= 1
+            self.stats["eager_steps"] += 1
+            self._tune(lbm)
+            ready = torch.cuda.Event()
+            ready.record(init)
+        slot.stream = self._pick_stream()
+        slot.stream.wait_event(ready)
+        self._top_up(slot)
+        return slot
 
     def prepare(self, requests):
         """Tune the launch-shape classes these requests will need, ahead of

@@ -99,3 +99,28 @@ def test_admission_respects_budget(mode):
     assert server.stats["max_used_bytes"] <= 2.5 * one
     with pytest.raises(ValueError):
         server.submit(Request(_cfg(19, (511, 511, 511), [P] * 6), 1))
+
+
+@pytest.mark.parametrize("mode", ["streams", "batched"])
+def test_rejected_request_does_not_stop_the_others(mode):
+    """A config the solver refuses (unknown velocity set: ValueError; a
+    NON_EQUILIBRIUM z face: NotImplementedError, the reference's error types)
+    comes back with the error on its request; the other requests finish with
+    the same result as alone."""
+    from funlbm_b200.serve import LBMServer, Request
+
+    good_cfg, good_steps = CASES[0]
+    bad_q = _cfg(19, (15, 15, 15), [P] * 6)
+    bad_q["flow"]["param_type"] = "D3Q17"
+    bad_face = _cfg(19, (15, 15, 15), [W, W, W, W, "NON_EQUILIBRIUM", W])
+    reqs = [Request(bad_q, 5), Request(good_cfg, good_steps), Request(bad_face, 5)]
+    server = LBMServer(budget_bytes=8e9, chunk=8, mode=mode, streams=4)
+    done = server.run(reqs, realtime=False)
+    assert len(done) == 3 and server.stats["rejected"] == 2
+    assert "ValueError" in reqs[0].result["error"]
+    assert "NotImplementedError" in reqs[2].result["error"]
+    ref = _alone(good_cfg, good_steps)
+    assert reqs[1].result["status"] == 0
+    for k in ("rho", "u"):
+        assert np.array_equal(to_np(reqs[1].result[k]), ref[k]), k
+    assert server.used == 0
