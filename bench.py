@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--serve-mode", default="streams", choices=["streams", "batched"])
     ap.add_argument("--serve-particles", type=int, default=1,
                     help="0: particle-free stream (for comparison)")
+    ap.add_argument("--case", default=None, choices=["sphere"],
+                    help="sphere: the single-sphere free-fall workload (161x65x65 D3Q19 fp32, "
+                         "walls, r = 8, rou 1.5, gl 2e-5) through LBMD3.run_step, IBM included")
     ap.add_argument("--shape", default=None,
                     help="fixed launch shape 'nodes,threads' (e.g. 2,128 or -1,256) instead of "
                          "the autotuner")
@@ -446,6 +449,55 @@ def run_serve(args):
     }
 
 
+def sphere_config(storage="fp32"):
+    """Single-sphere free-fall: size [160, 64, 64] (161 x 65 x 65 nodes, the
+    gravity axis is x), all faces WALL, mu 1/15 (tau 0.7), one sphere r = 8 at
+    (130, 32, 32) with density 1.5, gl = 2e-5."""
+    faces = ("input", "output", "back", "forward", "bottom", "top")
+    return {"device": "cuda", "log_per_steps": 10 ** 9, "file": {"per_steps": 10 ** 9},
+            "flow": {"size": [160, 64, 64], "param_type": "D3Q19",
+                     "param": {"mu": 0.0666667, "gl": 2e-5}, "precision": {"storage": storage},
+                     "boundary": {k: {"code": "WALL"} for k in faces}},
+            "particles": [{"type": "sphere", "r": 8, "rou": 1.5,
+                           "coord": {"center": [130.0, 32.0, 32.0]}}]}
+
+
+def run_case_sphere(args):
+    """Steps of the sphere free-fall through the public API (LBMD3.run_step:
+    interpolation, wall spring, rigid update, spreading, the fused step and
+    the marker update), timed with CUDA events on the launching stream."""
+    import torch
+
+    from funlbm_b200.lbm import LBMD3, Config
+
+    lbm = LBMD3(config=Config().from_json(sphere_config(args.storage)))
+    lbm.init()
+    for _ in range(args.warmup):
+        lbm.run_step(step=lbm.step)
+        lbm.step += 1
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        lbm.run_step(step=lbm.step)
+        lbm.step += 1
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    nodes = lbm.flow.n
+    p = lbm.particle_swarm.particles[0]
+    return {"metric": "MLUPS (D3Q19 %s sphere free-fall 161x65x65, IBM + rigid update)"
+                      % args.storage,
+            "value": nodes / (ms / 1e3) / 1e6, "unit": "MLUPS", "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "config": {"workload": "single sphere free-fall", "nodes": nodes,
+                       "markers": int(lbm.particle_swarm.struct().n_markers)},
+            "particle": {"cx": [float(v) for v in p.cx.tolist()],
+                         "cu": [float(v) for v in p.cu.tolist()]},
+            "status": int(lbm.check_status())}
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -511,6 +563,10 @@ def main():
 
     build.build()
     world, rank, local = dist_setup(args)
+    if args.case == "sphere":
+        if rank == 0:
+            print(json.dumps(run_case_sphere(args)), flush=True)
+        return 0
     if args.serve:
         if rank == 0:
             res = run_serve(args)
