@@ -386,49 +386,56 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles p) {
   const int pi = blockIdx.x;
-  __shared__ double R[9];
-  __shared__ float c[3];
-  if (threadIdx.x == 0) {
-    double v[3];
-    for (int k = 0; k < 3; ++k) {
-      const float ang = p.angle[3 * pi + k] + p.cw[3 * pi + k];
-      p.angle[3 * pi + k] = ang;
-      v[k] = ang;
-      c[k] = p.cx[3 * pi + k];
-    }
-    const double th = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    double s;
-    if (th <= 1e-3) {
-      const double t2 = th * th;
-      s = 0.5 - t2 / 48.0 + t2 * t2 / 3840.0;
-    } else {
-      s = sin(0.5 * th) / th;
-    }
-    double x = s * v[0], y = s * v[1], z = s * v[2], w = cos(0.5 * th);
-    const double nq = sqrt(x * x + y * y + z * z + w * w);
-    x /= nq;
-    y /= nq;
-    z /= nq;
-    w /= nq;
-    R[0] = 1 - 2 * (y * y + z * z);
-    R[1] = 2 * (x * y - z * w);
-    R[2] = 2 * (x * z + y * w);
-    R[3] = 2 * (x * y + z * w);
-    R[4] = 1 - 2 * (x * x + z * z);
-    R[5] = 2 * (y * z - x * w);
-    R[6] = 2 * (x * z - y * w);
-    R[7] = 2 * (y * z + x * w);
-    R[8] = 1 - 2 * (x * x + y * y);
-  }
-  __syncthreads();
   const int m0 = p.marker_offset[pi], m1 = p.marker_offset[pi + 1];
-  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double X = p.lagrange[3 * m], Y = p.lagrange[3 * m + 1], Z = p.lagrange[3 * m + 2];
+  // the first marker of this thread is loaded before the rotation is built,
+  // so the load latency overlaps it
+  int m = m0 + (int)threadIdx.x;
+  double X = 0.0, Y = 0.0, Z = 0.0;
+  if (m < m1) {
+    X = p.lagrange[3 * m];
+    Y = p.lagrange[3 * m + 1];
+    Z = p.lagrange[3 * m + 2];
+  }
+  // every thread builds the same rotation (no shared-memory broadcast)
+  double v[3];
+  float ang[3], c[3];
+  for (int k = 0; k < 3; ++k) {
+    ang[k] = p.angle[3 * pi + k] + p.cw[3 * pi + k];
+    v[k] = ang[k];
+    c[k] = p.cx[3 * pi + k];
+  }
+  const double th = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  double s;
+  if (th <= 1e-3) {
+    const double t2 = th * th;
+    s = 0.5 - t2 / 48.0 + t2 * t2 / 3840.0;
+  } else {
+    s = sin(0.5 * th) / th;
+  }
+  double x = s * v[0], y = s * v[1], z = s * v[2], w = cos(0.5 * th);
+  const double nq = sqrt(x * x + y * y + z * z + w * w);
+  x /= nq;
+  y /= nq;
+  z /= nq;
+  w /= nq;
+  const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w),     2 * (x * z + y * w),
+                       2 * (x * y + z * w),     1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                       2 * (x * z - y * w),     2 * (y * z + x * w),     1 - 2 * (x * x + y * y)};
+  for (; m < m1; m += kRigidThreads) {
     for (int k = 0; k < 3; ++k) {
       const double r = R[3 * k] * X + R[3 * k + 1] * Y + R[3 * k + 2] * Z;
       p.lx[3 * m + k] = (float)r + c[k];
     }
+    const int mn = m + kRigidThreads;
+    if (mn < m1) {
+      X = p.lagrange[3 * mn];
+      Y = p.lagrange[3 * mn + 1];
+      Z = p.lagrange[3 * mn + 2];
+    }
   }
+  __syncthreads();   // every thread has read the old angle
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) p.angle[3 * pi + k] = ang[k];
 }
 
 template <int Q>
