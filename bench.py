@@ -465,7 +465,9 @@ def sphere_config(storage="fp32"):
 def run_case_sphere(args):
     """Steps of the sphere free-fall through the public API (LBMD3.run_step:
     interpolation, wall spring, rigid update, spreading, the fused step and
-    the marker update), timed with CUDA events on the launching stream."""
+    the marker update), timed with CUDA events on the launching stream; then
+    the same number of steps through LBMD3.run_steps, which replays them from
+    captured CUDA graphs."""
     import torch
 
     from funlbm_b200.lbm import LBMD3, Config
@@ -485,12 +487,23 @@ def run_case_sphere(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    # the same steps through LBMD3.run_steps: plain steps replayed from
+    # captured CUDA graphs between logging / checkpoint steps
+    lbm.run_steps(args.warmup)
+    torch.cuda.synchronize()
+    e0.record()
+    lbm.run_steps(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_graphed = e0.elapsed_time(e1) / max(args.steps, 1)
     nodes = lbm.flow.n
     p = lbm.particle_swarm.particles[0]
     return {"metric": "MLUPS (D3Q19 %s sphere free-fall 161x65x65, IBM + rigid update)"
                       % args.storage,
             "value": nodes / (ms / 1e3) / 1e6, "unit": "MLUPS", "higher_is_better": True,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "graphed": {"value": nodes / (ms_graphed / 1e3) / 1e6, "ms_per_step": ms_graphed,
+                        "how": "LBMD3.run_steps (graph_steps = 32)"},
             "config": {"workload": "single sphere free-fall", "nodes": nodes,
                        "markers": int(lbm.particle_swarm.struct().n_markers)},
             "particle": {"cx": [float(v) for v in p.cx.tolist()],

@@ -14,7 +14,9 @@ reference's call sequence instead (``_compute_flow`` ->
 ``_handle_immersed_boundary`` -> ``_update_particles``), each method one
 kernel.  Keys added to the reference's config: ``fused`` (default true),
 ``log_per_steps`` (cadence of ``_log_step_info``; default 1 like the
-reference, which logs every step), ``ibm.mode`` (``reference`` = the
+reference, which logs every step), ``graph_steps`` (``run`` replays the
+fused steps between logging / checkpoint steps from captured CUDA graphs of
+up to this many steps; default 32, 0 = never), ``ibm.mode`` (``reference`` = the
 reference's last-writer-wins spreading, ``accumulate`` = summed spreading),
 ``flow.precision.storage``, ``flow.body_force``, ``flow.init_field``.
 """
@@ -54,6 +56,7 @@ class Config(BaseConfig):
         self.fused = True
         self.log_per_steps = 1
         self.ibm_mode = "reference"
+        self.graph_steps = 32
 
     def _from_json(self, config_json: dict, *args, **kwargs) -> "Config":
         self.dt = deep_get(config_json, "dt") or self.dt
@@ -71,6 +74,8 @@ class Config(BaseConfig):
         fused = deep_get(config_json, "fused")
         self.fused = True if fused is None else bool(fused)
         self.log_per_steps = int(deep_get(config_json, "log_per_steps") or self.log_per_steps)
+        gs = deep_get(config_json, "graph_steps")
+        self.graph_steps = self.graph_steps if gs is None else int(gs)
         self.ibm_mode = deep_get(config_json, "ibm.mode") or self.ibm_mode
         if self.ibm_mode not in ("reference", "accumulate"):
             raise ValueError("ibm.mode must be 'reference' or 'accumulate'")
@@ -113,14 +118,90 @@ class LBMBase:
     def run(self, max_steps: int = 1000000, *args, **kwargs) -> None:
         self.init()
         total_steps = min(max_steps, self.config.max_step)
-        for _ in range(total_steps):
+        self._run_loop(total_steps)
+
+    def run_steps(self, count: int) -> None:
+        """Advance ``count`` steps from ``self.step`` the way ``run`` does
+        (logging, checkpoints and status at their cadence, graph replays in
+        between) and leave ``self.step`` at the next step."""
+        if count <= 0:
+            return
+        last = self.step + count - 1
+        self._run_loop(last)
+        if self.run_status:
+            self.step = last + 1
+
+    def _run_loop(self, last):
+        while True:
+            quiet = self._quiet_steps(last)
+            if quiet >= 2:
+                self._advance_graphed(quiet)
             self.run_step(step=self.step)
             self._log_step_info(self.step)
             if self.run_status is False:
                 break
-            if self.step >= total_steps:
+            if self.step >= last:
                 break
             self.step += 1
+
+    def _quiet_steps(self, last):
+        """How many steps from self.step on are plain fused steps: not the
+        first (it enters the fused form), no logging, no checkpoint, not the
+        last one."""
+        gs = int(self.config.graph_steps or 0)
+        if gs < 2 or self.step <= 1 or not self._use_fused() or self.flow._mode != "fused":
+            return 0
+        s = self.step
+        L = max(1, int(self.config.log_per_steps))
+        P = max(1, int(self.config.file_config.per_steps))
+        nxt = min(last, -(-s // L) * L, -(-s // P) * P)
+        return max(0, nxt - s)
+
+    def _advance_graphed(self, count):
+        """Run `count` plain fused steps from captured graphs of up to
+        ``graph_steps`` steps (separate graphs before and after step 100, where
+        the interpolation's weight-sum check switches on: lbm/lbm3d.py:84),
+        eager steps for what is left over."""
+        end = self.step + count
+        while self.step < end:
+            rem = end - self.step
+            span = rem if self.step > 100 else min(rem, 101 - self.step)
+            n = min(int(self.config.graph_steps), span)
+            n -= n % 2
+            if n >= 2:
+                g = self._graph(n)
+                reps = span // n
+                for _ in range(reps):
+                    g.replay()
+                self.step += n * reps
+            else:
+                self._fused_step()
+                self.step += 1
+
+    def _graph(self, n):
+        """Captured n-step graph (n even) for the current buffer parity and
+        interpolation phase; the Python bookkeeping returns to the same
+        buffers after an even number of steps, so it replays any number of
+        times.  Captured on a side stream; nothing runs during capture."""
+        lat = self.flow.lattice
+        key = (n, self.step > 100, lat.cur, getattr(self, "_fi", 0))
+        cache = self.__dict__.setdefault("_graphs", {})
+        g = cache.get(key)
+        if g is None:
+            cap = self.__dict__.get("_graph_stream")
+            if cap is None:
+                cap = self._graph_stream = torch.cuda.Stream(device=self.device)
+            cap.wait_stream(torch.cuda.current_stream(self.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(cap):
+                g.capture_begin()
+                try:
+                    for _ in range(n):
+                        self._fused_step()
+                finally:
+                    g.capture_end()
+            cache[key] = g
+        return g
 
     def _log_step_info(self, *args, **kwargs) -> None:
         """lbm/base.py:105-144 at the ``log_per_steps`` cadence; also reads the
