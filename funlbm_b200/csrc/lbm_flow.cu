@@ -359,7 +359,7 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
   if (rc) return rc;
   const int bits = lat->storage == LBM_STORAGE_FP32 ? 32 : 16;
   if (lat->step_nodes != 0 && lat->step_nodes != LBM_STEP_ROWS &&
-      !step_shape_ok(lat->step_nodes, lat->nz, bits)) {
+      !step_shape_legal(lat->step_nodes, lat->nz, bits)) {
     set_error("lbm_flow_step: %d nodes per thread does not fit rows of %d nodes (%d-bit storage)",
               lat->step_nodes, lat->nz, bits);
     return LBM_ERR_INVALID;

@@ -163,6 +163,10 @@ struct Storage<LBM_STORAGE_BF16S> {
   }
 };
 
+// Raw 16 bits of one stored element.
+__device__ __forceinline__ unsigned short bits16(__half h) { return __half_as_ushort(h); }
+__device__ __forceinline__ unsigned short bits16(__nv_bfloat16 h) { return __bfloat16_as_ushort(h); }
+
 // Two consecutive stored elements <-> two working values (low element first).
 template <int S>
 __device__ __forceinline__ float2 work2(unsigned word);

@@ -220,17 +220,21 @@ __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0,
 // (fewer registers, more resident warps); for 4 and 8 the fully unpacked
 // form below keeps more independent work per thread and wins.  Same
 // arithmetic per node as every other shape.
-template <int Q, int S, bool FORCE, int NZ, bool COMPACT>
-__device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned t) {
+// ALIGNED = false: the pair starts at any index (rows of odd length), so
+// its elements are loaded and stored one by one and its nodes may lie in two
+// different force chunks.
+template <int Q, int S, bool FORCE, int NZ, bool COMPACT, bool ALIGNED = true>
+__device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsigned idx0) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
   static_assert(St::kBits == 16 && NZ % 2 == 0, "pairs of 16-bit elements");
+  static_assert(ALIGNED || NZ == 2, "unaligned pairs are single pairs");
   constexpr int kWords = NZ / 2;
-  const unsigned idx0 = t * NZ;
   if (idx0 >= (unsigned)a.g.n) return;
   int x, y, z0;
   const ChunkForce cf = chunk_force<FORCE>(a, idx0);
+  const ChunkForce cf1 = ALIGNED ? cf : chunk_force<FORCE>(a, idx0 + 1);
   a.dec(idx0, x, y, z0);
   constexpr bool kCompact = COMPACT;
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
@@ -249,7 +253,10 @@ __device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned
       constexpr int i = decltype(ic)::value;
       constexpr int ez = V::ez(i);
       const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
-      raw[i] = ld_words<kWords>(ps);
+      if constexpr (ALIGNED)
+        raw[i] = ld_words<kWords>(ps);
+      else
+        raw[i].w[0] = (unsigned)bits16(St::raw(ps)) | ((unsigned)bits16(St::raw(ps + 1)) << 16);
       if constexpr (ez > 0)
         extra[i] = St::raw(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx0 : ps - 1);
       if constexpr (ez < 0)
@@ -290,17 +297,29 @@ __device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned
     finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
                                 !row_in || za == 0 || za == a.g.nz - 1, cf, bad);
     finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
-                                !row_in || za + 1 == a.g.nz - 1, cf, bad);
+                                !row_in || za + 1 == a.g.nz - 1, cf1, bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        st_words(static_cast<T *>(a.p.dst[i]) + idx0 + 2 * pr,
-                 Words<1>{{put2<S>(f0[i], f1[i])}});
+        T *dst = static_cast<T *>(a.p.dst[i]) + idx0 + 2 * pr;
+        const unsigned word = put2<S>(f0[i], f1[i]);
+        if constexpr (ALIGNED) {
+          st_words(dst, Words<1>{{word}});
+        } else {
+          reinterpret_cast<unsigned short *>(dst)[0] = (unsigned short)(word & 0xffffu);
+          reinterpret_cast<unsigned short *>(dst)[1] = (unsigned short)(word >> 16);
+        }
       });
     }
   }
   report_bad(a.status, bad);
 }
+
+template <int Q, int S, bool FORCE, int NZ, bool COMPACT>
+__device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned t) {
+  step_vec_pairs_at<Q, S, FORCE, NZ, COMPACT, true>(a, t * NZ);
+}
+
 
 template <int Q, int S, bool FORCE, int NZ, bool COMPACT = compact_face_rows<Q, S, FORCE>()>
 __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned t) {
@@ -416,6 +435,24 @@ constexpr int vec_min_blocks() {
 template <int Q, int S, bool FORCE, int NZ, int TB>
 __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>())) k_step_vec(const StepArgs a) {
   step_vec_body<Q, S, FORCE, NZ>(a, blockIdx.x * TB + threadIdx.x);
+}
+
+// Rows of odd length in 16-bit storage: thread k of a row takes the node pair
+// (2k, 2k + 1) through the pair code with element-wise loads, and the last
+// thread of the row the single node nz - 1 through the one-node code.  Same
+// per-node arithmetic as every other shape.
+template <int Q, int S, bool FORCE, int TB>
+__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, 2, TB, FORCE>()))
+    k_step_odd(const StepArgs a, const FastDiv per_row, unsigned rows) {
+  const unsigned t = blockIdx.x * TB + threadIdx.x;
+  const unsigned row = fdiv(t, per_row);
+  if (row >= rows) return;
+  const unsigned z = 2u * (t - row * per_row.d);
+  const unsigned idx = row * (unsigned)a.g.nz + z;
+  if (z + 1u < (unsigned)a.g.nz)
+    step_vec_pairs_at<Q, S, FORCE, 2, compact_face_rows<Q, S, FORCE>(), false>(a, idx);
+  else
+    step_scalar_body<Q, S, FORCE>(a, idx);
 }
 
 // ---------------------------------------------------------------------------
@@ -655,6 +692,13 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
 // Launch shape of the fused step: nodes per thread (1 = scalar kernel, or
 // NZ consecutive z-nodes moved as 4 / 8 / 16-byte vectors, nz a multiple of
 // NZ) and threads per block.
+// Shapes lbm_flow_step accepts: the above, plus 2 nodes per thread for
+// 16-bit rows of odd length (k_step_odd).
+inline bool step_shape_ok(int nodes, int nz, int bits);
+inline bool step_shape_legal(int nodes, int nz, int bits) {
+  return step_shape_ok(nodes, nz, bits) || (nodes == 2 && bits == 16 && nz % 2 == 1 && nz >= 3);
+}
+
 inline bool step_shape_ok(int nodes, int nz, int bits) {
   if (nodes == 1) return true;
   if (nodes != 2 && nodes != 4 && nodes != 8) return false;
@@ -749,9 +793,25 @@ struct StepLauncher {
     else
       go_vec<NZ, 256>(a, force, s);
   }
+  template <bool FORCE, int TB>
+  static void go_odd_f(const StepArgs &a, cudaStream_t s) {
+    if constexpr (Storage<S>::kBits == 16) {
+      const unsigned per_row = (unsigned)(a.g.nz + 1) / 2;
+      const unsigned rows = (unsigned)(a.g.nx * a.g.ny);
+      const unsigned nb = blocks_for((long long)rows * per_row, TB);
+      k_step_odd<Q, S, FORCE, TB><<<nb, TB, 0, s>>>(a, make_fastdiv(per_row), rows);
+    }
+  }
+  static void go_odd(const StepArgs &a, bool force, int threads, cudaStream_t s) {
+    if (threads == 256)
+      force ? go_odd_f<true, 256>(a, s) : go_odd_f<false, 256>(a, s);
+    else
+      force ? go_odd_f<true, 128>(a, s) : go_odd_f<false, 128>(a, s);
+  }
   static int go(const StepArgs &a, bool force, int nodes, int threads, cudaStream_t s) {
     constexpr int bits = Storage<S>::kBits;
     if (nodes == LBM_STEP_ROWS) return go_tma(a, force, s);
+    const bool odd_pairs = bits == 16 && a.g.nz % 2 == 1 && a.g.nz >= 3;
     if (nodes == 0) {
       // measured on B200 at 512^3: 2 nodes per thread with 128-thread blocks
       // is the fastest shape for every velocity set and storage, except
@@ -759,8 +819,14 @@ struct StepLauncher {
       // are -- unforced only: the forced 4-node kernel spills (see
       // funlbm_b200.tune)
       const int want = (bits == 16 && Q == 19 && !force) ? 4 : 2;
-      nodes = step_shape_ok(want, a.g.nz, bits) ? want : step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
+      nodes = step_shape_ok(want, a.g.nz, bits)                ? want
+              : (step_shape_ok(2, a.g.nz, bits) || odd_pairs) ? 2
+                                                               : 1;
       threads = threads ? threads : 128;
+    }
+    if (nodes == 2 && odd_pairs) {
+      go_odd(a, force, threads, s);
+      return LBM_OK;
     }
     if (nodes == 2) {
       go_nz<2>(a, force, threads, s);

@@ -30,6 +30,8 @@ def shape_ok(nodes, nz, bits):
         return (nz * bits // 8) % 16 == 0 and nz >= 16
     if nodes * bits // 32 not in (1, 2, 4):
         return False
+    if nodes == 2 and bits == 16 and nz % 2 == 1 and nz >= 3:
+        return True                 # pairs within rows of odd length
     return nz % nodes == 0 and nz >= 2 * nodes
 
 

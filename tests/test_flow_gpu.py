@@ -395,3 +395,48 @@ def test_chunked_force_fields_agree_bitwise(q, storage):
     f = torch.empty(q * lat.n, device="cuda")
     lat.observe(None, f=f)
     assert not np.array_equal(to_np(f), ref)
+
+
+@pytest.mark.parametrize("q", [13, 19, 27])
+@pytest.mark.parametrize("storage", ["fp16s", "bf16s"])
+def test_odd_rows_agree_bitwise(q, storage):
+    """Rows of odd length in 16-bit storage: the pair kernel for odd rows
+    (element-wise loads, the last node of a row through the one-node code,
+    pairs that straddle a force chunk) gives the same bits as one node per
+    thread, with WALL_WITH_SPEED z faces and chunked force fields."""
+    from funlbm_b200.lattice import Lattice, make_force, tau_float32
+
+    shape = (10, 9, 15)
+    n = shape[0] * shape[1] * shape[2]
+    nch = (n + 31) // 32
+    rng = np.random.default_rng(11 + q)
+    kind = rng.integers(0, 4, nch)
+    ch_old = torch.tensor(((kind == 1) | (kind == 3)).astype(np.uint8), device="cuda")
+    ch_new = torch.tensor(((kind == 2) | (kind == 3)).astype(np.uint8), device="cuda")
+    node_kind = np.repeat(kind, 32)[:n]
+    f_old = 1e-4 * rng.standard_normal((n, 3)).astype(np.float32)
+    f_new = 1e-4 * rng.standard_normal((n, 3)).astype(np.float32)
+    f_old[~np.isin(node_kind, (1, 3))] = 0
+    f_new[~np.isin(node_kind, (2, 3))] = 0
+    F_old = torch.tensor(f_old.reshape(-1), device="cuda")
+    F_new = torch.tensor(f_new.reshape(-1), device="cuda")
+    force = make_force((0, 0, 0), (0, 0, 0), F_old, F_new, ch_old, ch_new)
+    codes = [1200, 11000, 11000, 1200, 1201, 1201]
+    uw = (0.02 * rng.standard_normal((6, 3))).tolist()
+    f0 = smooth_f0(q, shape, 0.04, q + 5)
+    f0_soa = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda")
+    results = {}
+    for nodes, threads in [(1, 256), (2, 128), (2, 256)]:
+        lat = Lattice(q, shape, codes, tau_float32(0.07), storage=storage, face_uw=uw,
+                      device="cuda")
+        lat.set_launch_shape(nodes, threads)
+        lat.init(f0_soa)
+        for _ in range(4):
+            lat.step(force)
+        assert lat.read_status() == 0
+        f = torch.empty(q * lat.n, device="cuda")
+        lat.observe(force, f=f)
+        results[(nodes, threads)] = to_np(f)
+    ref = results[(1, 256)]
+    for k, v in results.items():
+        assert np.array_equal(v, ref), (k, np.abs(v - ref).max())
