@@ -193,7 +193,7 @@ __host__ __device__ constexpr bool compact_face_rows() {
 // arithmetic.
 template <int Q, int S, bool FORCE>
 __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, int count, int x,
-                                               int y, int z0, ChunkForce cf) {
+                                               int y, int z0) {
   using St = Storage<S>;
   using T = typename St::T;
   const T *fa = static_cast<const T *>(a.fa);
@@ -202,7 +202,9 @@ __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0,
   for (int k = 0; k < count; ++k) {
     float f[Q];
     pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, a.face_rho_in, f);
-    finish_node<Q, FORCE, St::kDev>(a, f, idx0 + k, x, y, z0 + k, true, cf, bad);
+    // the nodes may lie in two chunks (pairs of odd-length rows)
+    finish_node<Q, FORCE, St::kDev>(a, f, idx0 + k, x, y, z0 + k, true,
+                                    chunk_force<FORCE>(a, idx0 + k), bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -240,7 +242,7 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {
     if (!row_in) {
-      face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0, cf);
+      face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0);
       return;
     }
     row_in = true;
@@ -340,7 +342,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {
     if (!row_in) {
-      face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0, cf);
+      face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0);
       return;
     }
     row_in = true;
