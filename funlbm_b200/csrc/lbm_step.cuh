@@ -442,7 +442,9 @@ __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>())) k
 // Rows of odd length in 16-bit storage: thread k of a row takes the node pair
 // (2k, 2k + 1) through the pair code with element-wise loads, and the last
 // thread of the row the single node nz - 1 through the one-node code.  Same
-// per-node arithmetic as every other shape.
+// per-node arithmetic as every other shape.  Measured on B200 it beats one
+// node per thread only for unforced D3Q19 (+7 % at 257^3) and loses for
+// D3Q27, so it is a tuner candidate, not a default.
 template <int Q, int S, bool FORCE, int TB>
 __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, 2, TB, FORCE>()))
     k_step_odd(const StepArgs a, const FastDiv per_row, unsigned rows) {
@@ -821,9 +823,9 @@ struct StepLauncher {
       // are -- unforced only: the forced 4-node kernel spills (see
       // funlbm_b200.tune)
       const int want = (bits == 16 && Q == 19 && !force) ? 4 : 2;
-      nodes = step_shape_ok(want, a.g.nz, bits)                ? want
-              : (step_shape_ok(2, a.g.nz, bits) || odd_pairs) ? 2
-                                                               : 1;
+      // (rows of odd length: one node per thread; the odd-row pair kernel
+      // is only a tuner candidate -- measured no faster in general)
+      nodes = step_shape_ok(want, a.g.nz, bits) ? want : step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
       threads = threads ? threads : 128;
     }
     if (nodes == 2 && odd_pairs) {
