@@ -163,8 +163,16 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   }
 }
 
+// Register cap of the one-node kernel (resident blocks per SM asked of the
+// compiler, 0 = none): 16-bit D3Q19 at 48 registers (5 blocks of 256; a few
+// spilled words) -- the kernel rows of odd length run in 16-bit storage.
+template <int Q, int S>
+constexpr int scalar_min_blocks() {
+  return (Storage<S>::kBits == 16 && Q == 19) ? 5 : 0;
+}
+
 template <int Q, int S, bool FORCE>
-__global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
+__global__ void __launch_bounds__(kThreads, (scalar_min_blocks<Q, S>())) k_step(const StepArgs a) {
   step_scalar_body<Q, S, FORCE>(a, blockIdx.x * kThreads + threadIdx.x);
 }
 
