@@ -74,9 +74,13 @@ typedef struct lbm_lattice {
   const double *neq_profile; /* device [ny*nz] duct profile init_u / u_max (float64, */
                              /* as cul_u returns it); NULL unless face[0] is NEQ    */
   int32_t step_nodes;     /* launch shape of lbm_flow_step: consecutive z-nodes per  */
-                          /* thread (1, 2, 4, 8), LBM_STEP_ROWS (whole z-rows staged */
-                          /* in shared memory by TMA bulk copies), 0 = default      */
-  int32_t step_threads;   /* threads per block (128 or 256; 0 = 256)                */
+                          /* thread (1, 2, 4, 8; nz a multiple of it, except 2 for  */
+                          /* 16-bit rows of odd length: pairs within rows),         */
+                          /* LBM_STEP_ROWS (whole z-rows staged in shared memory by */
+                          /* TMA bulk copies), 0 = default (measured best per Q /   */
+                          /* storage / forcing)                                     */
+  int32_t step_threads;   /* threads per block (128 or 256; 0 = 128 with the        */
+                          /* default shape, else 256)                               */
 } lbm_lattice;
 
 /* Forcing seen by one step: FOL = uniform + field.  `uniform` is a body force
