@@ -35,6 +35,31 @@ def shape_ok(nodes, nz, bits):
     return nz % nodes == 0 and nz >= 2 * nodes
 
 
+def default_shape(q, storage, nz, forced=False):
+    """The launch shape lbm_flow_step uses when none is set (measured best at
+    512^3): 2 nodes per thread with 128 threads, 4 for unforced D3Q19 in
+    16-bit storage, one node per thread where rows allow no vector."""
+    bits = 32 if storage == "fp32" else 16
+    want = 4 if (bits == 16 and q == 19 and not forced) else 2
+    for nodes in (want, 2):
+        if nz % nodes == 0 and nz >= 2 * nodes:
+            return (nodes, 128)
+    return (1, 256)
+
+
+# A candidate replaces the default shape only if its proxy timing is this much
+# faster: short proxy timings scatter by a few percent, and the default is the
+# measured best at full size.
+MARGIN = 0.03
+
+
+def _pick(timings, default):
+    best = min(timings, key=timings.get)
+    if default in timings and timings[default] <= timings[best] * (1.0 + MARGIN):
+        return default
+    return best
+
+
 def tune(lat, force=None, iters=6, warmup=2, verbose=False):
     """Choose (nodes per thread, threads per block) for ``lat`` and store it
     in its descriptor.  Returns the choice and the timings in ms per step."""
@@ -69,7 +94,7 @@ def tune(lat, force=None, iters=6, warmup=2, verbose=False):
         timings[(nodes, threads)] = start.elapsed_time(stop) / iters
     proxy.release()
     del proxy
-    choice = min(timings, key=timings.get)
+    choice = _pick(timings, default_shape(lat.q, lat.storage, nz, force is not None))
     if verbose:
         for k, v in sorted(timings.items(), key=lambda kv: kv[1]):
             print("tune q=%d %s %dx%dx%d (proxy nx=%d): nodes=%d threads=%d  %.4f ms"
@@ -141,7 +166,7 @@ def tune_class_of(q, storage, nz, forced, device="cuda", iters=6, warmup=2):
         timings[(nodes, threads)] = start.elapsed_time(stop) / iters
     proxy.release()
     del proxy
-    _CLASS_CACHE[key] = min(timings, key=timings.get)
+    _CLASS_CACHE[key] = _pick(timings, default_shape(q, storage, pnz, forced))
     return _CLASS_CACHE[key]
 
 

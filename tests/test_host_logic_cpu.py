@@ -72,3 +72,15 @@ def test_added_config_keys():
     assert c.ibm_mode == "accumulate" and c.flow_config.storage == "bf16s"
     with pytest.raises(ValueError):
         Config().from_json({"ibm": {"mode": "sum"}})
+
+
+def test_tuner_keeps_the_default_within_its_margin():
+    assert tune.default_shape(19, "fp32", 512) == (2, 128)
+    assert tune.default_shape(19, "fp16s", 512) == (4, 128)
+    assert tune.default_shape(19, "fp16s", 512, forced=True) == (2, 128)
+    assert tune.default_shape(27, "bf16s", 514) == (2, 128)
+    assert tune.default_shape(19, "fp32", 65) == (1, 256)
+    t = {(1, 256): 3.08, (2, 128): 3.10, (4, 128): 3.4}
+    assert tune._pick(t, (2, 128)) == (2, 128)          # within 3 %: keep the default
+    t[(1, 256)] = 2.9
+    assert tune._pick(t, (2, 128)) == (1, 256)          # clearly faster: take it
