@@ -110,8 +110,6 @@ SIGNATURES = {
     "lbm_moments": (I, [_LAT, _P, _P, _P, _P, _P, _P, _P]),
     "lbm_add_force": (I, [_LAT, _P, _P, _P, _P]),
     "ibm_interpolate": (I, [_LAT, _P, _FORCE, _P, _P, _P, _PART, F, ctypes.c_int32, _P, _P]),
-    "ibm_interpolate_halo": (I, [_LAT, _P, _FORCE, _P, _PART, F, ctypes.c_int32, _P, _P, _P, _P,
-                                 _P, _P, _P]),
     "rigid_wall_and_update": (I, [_LAT, _PART, ctypes.c_int32, F, F, F, F, _P]),
     "ibm_spread": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P, _P]),
     "ibm_spread_noalloc": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P]),

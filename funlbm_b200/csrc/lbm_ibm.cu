@@ -452,84 +452,6 @@ struct RunInterp {
   }
 };
 
-// ---------------------------------------------------------------------------
-// Interpolation with the moments taken once per stencil node.  Neighbouring
-// markers share most of their 4 x 4 x 4 stencils, so on a marked surface each
-// node lies in many stencils; k_interp on populations recomputes its moments
-// for every one.  Here (1) every (marker, slot) claims its node in the claim
-// array and the first claim appends the node to a list, (2) the moments of
-// each listed node are taken once, with k_interp's code, into scratch
-// fields, (3) k_interp runs on those fields (its u / rho path: the same
-// values, so the same bits), (4) the claims are released.
-// ---------------------------------------------------------------------------
-struct HaloArgs {
-  Geom g;
-  NodeDecomp dec;
-  const void *fa;
-  float go[3];
-  const float *fol_old;
-  const float *face_rho_in;
-  lbm_particles p;
-  StepPlanes planes;
-  float *u, *rho;
-  int32_t *owner, *list, *count;
-};
-
-__global__ void __launch_bounds__(kIbmThreads) k_halo_claim(const HaloArgs a) {
-  const int mk = threadIdx.x / kStencil, slot = threadIdx.x % kStencil;
-  const int m = blockIdx.x * kMarkersPerBlock + mk;
-  if (m >= a.p.n_markers) return;
-  const float l[3] = {a.p.lx[3 * m], a.p.lx[3 * m + 1], a.p.lx[3 * m + 2]};
-  int x, y, z;
-  float w;
-  if (!stencil_slot(a.g, l, slot, x, y, z, w)) return;
-  const int32_t idx = (int32_t)(((long long)x * a.g.ny + y) * a.g.nz + z);
-  if (atomicCAS(a.owner + idx, -1, 1) == -1) a.list[atomicAdd(a.count, 1)] = idx;
-}
-
-template <int Q, int S>
-__global__ void __launch_bounds__(256) k_halo_moments(const HaloArgs a) {
-  const int t = blockIdx.x * 256 + threadIdx.x;
-  if (t >= *a.count) return;
-  const unsigned idx = (unsigned)a.list[t];
-  int x, y, z;
-  a.dec(idx, x, y, z);
-  const typename Storage<S>::T *fa = static_cast<const typename Storage<S>::T *>(a.fa);
-  float f[Q];
-  if (x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1)
-    pull_row_node<Q, S, false>(a.planes, a.g, a.face_rho_in, idx, x, y, z, f);
-  else
-    pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
-  float fx = a.go[0], fy = a.go[1], fz = a.go[2];
-  if (a.fol_old != nullptr) {
-    fx += a.fol_old[3 * (long long)idx];
-    fy += a.fol_old[3 * (long long)idx + 1];
-    fz += a.fol_old[3 * (long long)idx + 2];
-  }
-  float rho, ux, uy, uz;
-  moments<Q>(f, fx, fy, fz, on_any_face(a.g, x, y, z), rho, ux, uy, uz);
-  a.rho[idx] = rho;
-  a.u[3 * (long long)idx] = ux;
-  a.u[3 * (long long)idx + 1] = uy;
-  a.u[3 * (long long)idx + 2] = uz;
-}
-
-__global__ void k_halo_release(const HaloArgs a) {
-  const int t = blockIdx.x * 256 + threadIdx.x;
-  if (t < *a.count) a.owner[a.list[t]] = -1;
-}
-
-template <int Q>
-struct RunHaloMoments {
-  static void run(const HaloArgs &a, int storage, unsigned nb, cudaStream_t s) {
-    switch (storage) {
-      case LBM_STORAGE_FP32: k_halo_moments<Q, LBM_STORAGE_FP32><<<nb, 256, 0, s>>>(a); break;
-      case LBM_STORAGE_FP16S: k_halo_moments<Q, LBM_STORAGE_FP16S><<<nb, 256, 0, s>>>(a); break;
-      default: k_halo_moments<Q, LBM_STORAGE_BF16S><<<nb, 256, 0, s>>>(a); break;
-    }
-  }
-};
-
 static int check_particles(const lbm_particles *pt, const char *who) {
   if (pt == nullptr || pt->n_particles < 0 || pt->n_markers < 0) {
     set_error("%s: bad particle description", who);
@@ -632,69 +554,6 @@ int ibm_interpolate(const lbm_lattice *lat, const void *fa, const lbm_force *for
     case 19: return RunInterp<19>::run(a, lat->storage, (cudaStream_t)stream);
     default: return RunInterp<27>::run(a, lat->storage, (cudaStream_t)stream);
   }
-}
-
-int ibm_interpolate_halo(const lbm_lattice *lat, const void *fa, const lbm_force *force,
-                         const float *face_rho_in, const lbm_particles *pt, float dt, int32_t step,
-                         uint32_t *status, float *u_scratch, float *rho_scratch, int32_t *owner,
-                         int32_t *list, int32_t *count, void *stream) {
-  int rc = check_lattice(lat);
-  if (rc) return rc;
-  if ((rc = check_particles(pt, "ibm_interpolate_halo"))) return rc;
-  if (!(dt > 0.f)) {
-    set_error("ibm_interpolate_halo: dt must be positive");
-    return LBM_ERR_INVALID;
-  }
-  if (fa == nullptr || u_scratch == nullptr || rho_scratch == nullptr || owner == nullptr ||
-      list == nullptr || count == nullptr) {
-    set_error("ibm_interpolate_halo: needs the populations and every scratch buffer");
-    return LBM_ERR_INVALID;
-  }
-  if (any_face(lat, LBM_BC_NON_EQUILIBRIUM)) {
-    set_error("ibm_interpolate_halo: NON_EQUILIBRIUM faces need ibm_interpolate on the fields");
-    return LBM_ERR_UNSUPPORTED;
-  }
-  if (any_face(lat, LBM_BC_WALL_WITH_SPEED) && face_rho_in == nullptr) {
-    set_error("ibm_interpolate_halo: WALL_WITH_SPEED faces need face_rho_in");
-    return LBM_ERR_INVALID;
-  }
-  if (pt->n_markers == 0) return LBM_OK;
-  cudaStream_t s = (cudaStream_t)stream;
-  HaloArgs h;
-  memset(&h, 0, sizeof(h));
-  h.g = make_geom(lat);
-  h.dec = make_decomp(h.g);
-  h.fa = fa;
-  fill_step_planes(h.g, lat->q, lat->storage, fa, nullptr, h.planes);
-  if (force != nullptr) {
-    for (int k = 0; k < 3; ++k) h.go[k] = force->old_uniform[k];
-    h.fol_old = force->old_field;
-  }
-  h.face_rho_in = face_rho_in;
-  h.p = *pt;
-  h.u = u_scratch;
-  h.rho = rho_scratch;
-  h.owner = owner;
-  h.list = list;
-  h.count = count;
-  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int32_t), s);
-  if (e != cudaSuccess) return fail_cuda(e, "ibm_interpolate_halo");
-  const unsigned nbm = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
-  const unsigned nbl = (unsigned)(((long long)pt->n_markers * kStencil + 255) / 256);
-  k_halo_claim<<<nbm, kIbmThreads, 0, s>>>(h);
-  switch (lat->q) {
-    case 13: RunHaloMoments<13>::run(h, lat->storage, nbl, s); break;
-    case 15: RunHaloMoments<15>::run(h, lat->storage, nbl, s); break;
-    case 19: RunHaloMoments<19>::run(h, lat->storage, nbl, s); break;
-    default: RunHaloMoments<27>::run(h, lat->storage, nbl, s); break;
-  }
-  LBM_LAUNCH_CHECK("ibm_interpolate_halo");
-  rc = ibm_interpolate(lat, nullptr, force, nullptr, u_scratch, rho_scratch, pt, dt, step,
-                       status, stream);
-  if (rc) return rc;
-  k_halo_release<<<nbl, 256, 0, s>>>(h);
-  LBM_LAUNCH_CHECK("ibm_interpolate_halo");
-  return LBM_OK;
 }
 
 int rigid_wall_and_update(const lbm_lattice *lat, const lbm_particles *pt, int32_t what, float dt,

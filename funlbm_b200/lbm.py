@@ -40,11 +40,6 @@ from .particle import ParticleConfig, ParticleSwarm, create_particle_swarm
 logger = logging.getLogger("funlbm_b200")
 
 
-# From this many markers on, interpolation takes the moments once per stencil
-# node (ibm_interpolate_halo) instead of once per (marker, stencil slot).
-HALO_MIN_MARKERS = 4096
-
-
 class Config(BaseConfig):
     """lbm/base.py:17-40 plus the keys listed in the module docstring."""
 
@@ -384,18 +379,6 @@ class LBMD3(LBMBase):
         return _lib.stream_of(torch, self.device)
 
     # -- IBM buffers ------------------------------------------------------------
-    def _halo_buffers(self, n_markers):
-        """Scratch of ibm_interpolate_halo: u [3n], rho [n], node list
-        [64 * markers], count [1] (allocated once, kept)."""
-        halo = self.__dict__.get("_halo")
-        if halo is None or halo[2].numel() < 64 * n_markers:
-            n, dev = self.flow.n, self.device
-            halo = (torch.empty(3 * n, device=dev), torch.empty(n, device=dev),
-                    torch.empty(64 * n_markers, dtype=torch.int32, device=dev),
-                    torch.zeros(1, dtype=torch.int32, device=dev))
-            self._halo = halo
-        return halo
-
     def _ensure_ibm(self):
         if self._fol is not None:
             return
@@ -452,18 +435,9 @@ class LBMD3(LBMBase):
             sw = self.particle_swarm
             st = ctypes.byref(sw.struct())
             f_int = make_force(old_uniform=g_old, old_field=F_old)
-            n_markers = int(sw.struct().n_markers)
-            if n_markers >= HALO_MIN_MARKERS:
-                # many markers: moments once per stencil node (same result)
-                halo = self._halo_buffers(n_markers)
-                call("ibm_interpolate_halo", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]),
-                     ctypes_ref(f_int), ptr(lat.face_rho[lat.cur]), st, float(self.config.dt),
-                     int(self.step), ptr(self._status_ibm), ptr(halo[0]), ptr(halo[1]),
-                     ptr(self._owner), ptr(halo[2]), ptr(halo[3]), s)
-            else:
-                call("ibm_interpolate", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]),
-                     ctypes_ref(f_int), ptr(lat.face_rho[lat.cur]), None, None, st,
-                     float(self.config.dt), int(self.step), ptr(self._status_ibm), s)
+            call("ibm_interpolate", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]), ctypes_ref(f_int),
+                 ptr(lat.face_rho[lat.cur]), None, None, st, float(self.config.dt),
+                 int(self.step), ptr(self._status_ibm), s)
             call("rigid_wall_and_update", ctypes_ref(lat.desc), st,
                  _lib.RIGID_WALL | _lib.RIGID_UPDATE, float(self.config.dt),
                  float(self.config.dx), float(self.config.flow_config.gl), 1.0, s)

@@ -217,18 +217,6 @@ int ibm_interpolate(const lbm_lattice *lat, const void *fa, const lbm_force *for
                     const lbm_particles *pt, float dt, int32_t step, uint32_t *status,
                     void *stream);
 
-/* ibm_interpolate on populations with the moments taken once per stencil
- * node rather than once per (marker, stencil slot) -- neighbouring markers
- * share most of their stencils; same result, bit for bit.  Caller-owned
- * scratch: u_scratch [3n] and rho_scratch [n] floats (contents overwritten
- * where markers reach), owner [n] int32 at rest (-1 everywhere; the claim
- * array of ibm_spread, left at rest), list [64 * n_markers] int32 and
- * count [1] int32 (set here).  Worth it from a few thousand markers on. */
-int ibm_interpolate_halo(const lbm_lattice *lat, const void *fa, const lbm_force *force,
-                         const float *face_rho_in, const lbm_particles *pt, float dt,
-                         int32_t step, uint32_t *status, float *u_scratch, float *rho_scratch,
-                         int32_t *owner, int32_t *list, int32_t *count, void *stream);
-
 /* LBMD3.particle_to_wall (lbm/lbm3d.py:121-167) and
  * Particle.update_from_lar (particle/base/base.py:120-151) for all particles:
  * the spring force on the six extreme markers (what & 1), then force / torque

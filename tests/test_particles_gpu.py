@@ -15,7 +15,7 @@ import pytest
 import torch
 
 from oracle import lbm_oracle as O
-from tests.gpu_util import init_with, lbm_config, rel_err, require_cuda, run, smooth_f0, to_np
+from tests.gpu_util import init_with, lbm_config, rel_err, require_cuda, run, to_np
 
 pytestmark = pytest.mark.gpu
 
@@ -201,90 +201,5 @@ def test_run_with_graphs_matches_eager():
         out.append((to_np(lbm.flow.rou), to_np(lbm.flow.u), to_np(p.cx), to_np(p.cw)))
         if gs:
             assert len(lbm._graphs) >= 2          # before and after step 100
-    for a, b in zip(*out):
-        assert np.array_equal(a, b)
-
-
-@pytest.mark.parametrize("storage", ["fp32", "fp16s"])
-def test_halo_interpolation_matches_direct(storage):
-    """ibm_interpolate_halo (moments once per stencil node) writes the same
-    lu / lF / lrou bits as ibm_interpolate on populations, with
-    WALL_WITH_SPEED faces and a previous force field, two calls in a row,
-    and leaves the claim array at rest."""
-    import ctypes
-
-    from funlbm_b200 import _lib
-    from funlbm_b200._lib import ptr
-    from funlbm_b200.lattice import Lattice, make_force, tau_float32
-    from funlbm_b200.particle import ParticleConfig, ParticleSwarm
-
-    q, shape = 19, (34, 30, 32)
-    codes = [1201, 1200, 11000, 11000, 1201, 1200]
-    rng = np.random.default_rng(5)
-    uw = (0.02 * rng.standard_normal((6, 3))).tolist()
-    lat = Lattice(q, shape, codes, tau_float32(0.07), storage=storage, face_uw=uw, device="cuda")
-    f0 = smooth_f0(q, shape, 0.04, 9)
-    lat.init(torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda"))
-    lat.face_rho[lat.cur].copy_(torch.tensor(1.0 + 0.01 * rng.standard_normal(
-        lat.face_rho[lat.cur].numel()), dtype=torch.float32, device="cuda"))
-    cfgs = [ParticleConfig().from_json({"type": "sphere", "r": r, "coord": {"center": c}})
-            for r, c in ((5, [10.3, 12.1, 11.7]), (4, [22.6, 16.4, 17.9]), (3, [16.2, 8.8, 24.1]))]
-    sw = ParticleSwarm(cfgs, device="cuda")
-    sw.init()
-    sw.update()
-    n = lat.n
-    F_old = torch.tensor(1e-4 * rng.standard_normal(3 * n), dtype=torch.float32, device="cuda")
-    force = make_force((1e-6, 0, -2e-6), (0, 0, 0), F_old, None)
-    status = torch.zeros(1, dtype=torch.int32, device="cuda")
-    owner = torch.full((n,), -1, dtype=torch.int32, device="cuda")
-    nm = int(sw.struct().n_markers)
-    u_s, rho_s = torch.empty(3 * n, device="cuda"), torch.empty(n, device="cuda")
-    lst = torch.empty(64 * nm, dtype=torch.int32, device="cuda")
-    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
-    s = lat.stream()
-    for call in range(2):
-        if call:
-            sw.cx.add_(torch.tensor([0.37, -0.21, 0.44], device="cuda"))
-            sw.update()
-        st = ctypes.byref(sw.struct())
-        _lib.call("ibm_interpolate", ctypes.byref(lat.desc), ptr(lat.buf[lat.cur]),
-                  ctypes.byref(force), ptr(lat.face_rho[lat.cur]), None, None, st, 1.0, 150,
-                  ptr(status), s)
-        direct = [to_np(getattr(sw, k)).copy() for k in ("lu", "lF", "lrou")]
-        _lib.call("ibm_interpolate_halo", ctypes.byref(lat.desc), ptr(lat.buf[lat.cur]),
-                  ctypes.byref(force), ptr(lat.face_rho[lat.cur]), st, 1.0, 150, ptr(status),
-                  ptr(u_s), ptr(rho_s), ptr(owner), ptr(lst), ptr(cnt), s)
-        halo = [to_np(getattr(sw, k)) for k in ("lu", "lF", "lrou")]
-        for a, b in zip(direct, halo):
-            assert np.array_equal(a, b), call
-        assert 0 < int(cnt.item()) < 64 * nm          # shared stencil nodes counted once
-        assert bool((owner == -1).all())
-    assert int(status.item()) == 0
-
-
-def test_run_with_halo_interpolation_matches(monkeypatch):
-    """A particle run with every interpolation through the halo path gives
-    the same state bit for bit."""
-    from funlbm_b200 import lbm as L
-
-    faces = ("input", "output", "back", "forward", "bottom", "top")
-    cfg = {"device": "cuda", "log_per_steps": 10 ** 9, "file": {"per_steps": 10 ** 9},
-           "flow": {"size": [30, 22, 24], "param_type": "D3Q19", "param": {"mu": 0.08, "gl": 1e-3},
-                    "boundary": {k: {"code": "WALL"} for k in faces}},
-           "particles": [{"type": "sphere", "r": 3, "rou": 1.3, "coord": {"center": [12.0, 11.0, 12.0]}},
-                         {"a": 4, "b": 3, "c": 3, "rou": 1.2,
-                          "coord": {"center": [20.0, 10.0, 12.5], "alpha": 0.3, "beta": 0.2,
-                                    "gamma": 0.1}}]}
-    out = []
-    for threshold in (10 ** 9, 0):
-        monkeypatch.setattr(L, "HALO_MIN_MARKERS", threshold)
-        lbm = L.LBMD3(config=L.Config().from_json(cfg))
-        lbm.init()
-        for _ in range(25):
-            lbm.run_step(step=lbm.step)
-            lbm.step += 1
-        ps = lbm.particle_swarm.particles
-        out.append([to_np(lbm.flow.rou), to_np(lbm.flow.u)] + [to_np(p.cx) for p in ps])
-        assert (threshold == 0) == ("_halo" in lbm.__dict__)
     for a, b in zip(*out):
         assert np.array_equal(a, b)
