@@ -21,6 +21,7 @@ LBM_STATUS_RHO_BAD = 0x1
 LBM_STATUS_U_BAD = 0x2
 LBM_STATUS_STENCIL_EMPTY = 0x4
 LBM_STATUS_WAIT_TIMEOUT = 0x8
+LBM_STATUS_DRAIN_FAILED = 0x10
 
 STORAGE = {"fp32": 0, "fp16s": 1, "bf16s": 2}
 SPREAD_NOALLOC_MAX_NODES = 1 << 22
@@ -114,6 +115,7 @@ SIGNATURES = {
     "ibm_spread": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P, _P]),
     "ibm_spread_noalloc": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P]),
     "rigid_update_markers": (I, [_PART, _P]),
+    "lbm_debug_set_wait_limit": (None, [ctypes.c_int64]),
     "lbm_last_error": (ctypes.c_char_p, []),
     "lbm_version": (ctypes.c_char_p, []),
 }

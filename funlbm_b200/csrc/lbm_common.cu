@@ -1,4 +1,5 @@
 // Error reporting, lattice validation and Geom construction for the C ABI.
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -10,7 +11,10 @@ namespace lbm {
 
 namespace {
 thread_local char g_msg[512] = "";
+std::atomic<unsigned> g_tma_wait_polls{kTmaWaitPollsDefault};
 }
+
+unsigned tma_wait_polls() { return g_tma_wait_polls.load(std::memory_order_relaxed); }
 
 void set_error(const char *fmt, ...) {
   va_list ap;
@@ -160,5 +164,12 @@ size_t lbm_face_plane_floats(const lbm_lattice *lat) {
 }
 
 int lbm_lattice_check(const lbm_lattice *lat) { return lbm::check_lattice(lat); }
+
+void lbm_debug_set_wait_limit(int64_t polls) {
+  const unsigned v = polls < 0 ? lbm::kTmaWaitPollsDefault
+                     : polls > (int64_t)lbm::kTmaWaitPollsDefault ? lbm::kTmaWaitPollsDefault
+                                                                   : (unsigned)polls;
+  lbm::g_tma_wait_polls.store(v, std::memory_order_relaxed);
+}
 
 }  // extern "C"

@@ -479,11 +479,17 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_owner_mu;
 int32_t *g_owner_addr[kMaxDevices] = {};
+// whether the array on a device holds -1 everywhere between calls: false
+// until the first reference-mode call resets it (__device__ memory starts at
+// 0), and again after a call whose launches failed part-way
+bool g_owner_clean[kMaxDevices] = {};
 }  // namespace
 
 // Device address of g_spread_owner on the current device, looked up once per
-// device (the first call on a device does this set-up).
-static int owner_scratch(int32_t **out) {
+// device (the first call on a device does this set-up), and whether the
+// array still needs its one-time reset to -1.  The cached address belongs to
+// the device's current primary context: after cudaDeviceReset it is stale.
+static int owner_scratch(int32_t **out, int *dev_out, bool *clean) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail_cuda(e, "ibm_spread_noalloc");
@@ -499,7 +505,14 @@ static int owner_scratch(int32_t **out) {
     g_owner_addr[dev] = static_cast<int32_t *>(p);
   }
   *out = g_owner_addr[dev];
+  *dev_out = dev;
+  *clean = g_owner_clean[dev];
   return LBM_OK;
+}
+
+static void owner_mark(int dev, bool clean) {
+  std::lock_guard<std::mutex> lock(g_owner_mu);
+  g_owner_clean[dev] = clean;
 }
 
 }  // namespace lbm
@@ -660,11 +673,10 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
     return LBM_ERR_INVALID;
   }
   int32_t *owner = nullptr;
-  if ((rc = owner_scratch(&owner))) return rc;
+  int dev = 0;
+  bool clean = false;
+  if ((rc = owner_scratch(&owner, &dev, &clean))) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  // the array keeps whatever the previous call left: reset the part used
-  k_owner_reset<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, s>>>(owner, n);
-  LBM_LAUNCH_CHECK("ibm_spread_noalloc");
   SpreadArgs a;
   a.g = make_geom(lat);
   a.p = *pt;
@@ -677,13 +689,25 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
   if (pt->n_markers == 0) return LBM_OK;
   const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
   if (mode == 0) {
+    // the claim passes need -1 in every slot they touch; the release pass
+    // restores it, so only the first reference-mode call on a device (or
+    // one after a failed call) resets the whole array
+    owner_mark(dev, false);
+    if (!clean) {
+      k_owner_reset<<<(unsigned)std::min<long long>(
+                          (LBM_SPREAD_NOALLOC_MAX_NODES + 255) / 256, 4096),
+                      256, 0, s>>>(owner, LBM_SPREAD_NOALLOC_MAX_NODES);
+      LBM_LAUNCH_CHECK("ibm_spread_noalloc");
+    }
     k_spread<0><<<nb, kIbmThreads, 0, s>>>(a);
     k_spread<1><<<nb, kIbmThreads, 0, s>>>(a);
     k_spread<2><<<nb, kIbmThreads, 0, s>>>(a);
+    LBM_LAUNCH_CHECK("ibm_spread_noalloc");
+    owner_mark(dev, true);
   } else {
     k_spread<3><<<nb, kIbmThreads, 0, s>>>(a);
+    LBM_LAUNCH_CHECK("ibm_spread_noalloc");
   }
-  LBM_LAUNCH_CHECK("ibm_spread_noalloc");
   return LBM_OK;
 }
 

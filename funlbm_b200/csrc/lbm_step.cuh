@@ -527,17 +527,21 @@ __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>()))
 // pulled from global memory with the full face rules.  Bytes in flight are
 // bounded by shared memory, not registers -- what the 16-bit storage needs
 // to reach HBM bandwidth.  Every barrier wait is bounded; a timeout sets
-// LBM_STATUS_WAIT_TIMEOUT and the CTA drains its copies (bounded) and stops.
+// LBM_STATUS_WAIT_TIMEOUT and the CTA drains its copies (bounded by the
+// default limit) and stops; a drain that also times out sets
+// LBM_STATUS_DRAIN_FAILED.
 // ---------------------------------------------------------------------------
 constexpr int kTmaThreads = 256;
-constexpr unsigned kTmaWaitPolls = 1u << 24;
+constexpr unsigned kTmaWaitPolls = kTmaWaitPollsDefault;
 
 struct TmaPlan {
   int rows_per_stage;
   int stages;
   unsigned row_bytes;
   long long groups;
+  unsigned wait_polls;   // limit of the consumer waits (the drain keeps kTmaWaitPolls)
 };
+
 
 // working value(s) of one / two staged elements
 template <int S>
@@ -623,7 +627,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
     if (g >= p.groups) break;
     const int s = (int)(k % p.stages);
     const unsigned par = (unsigned)((k / p.stages) & 1);
-    const bool ok = mbar_wait_bounded(&bars[s], par, kTmaWaitPolls);
+    const bool ok = mbar_wait_bounded(&bars[s], par, p.wait_polls);
     if (__syncthreads_or(!ok)) {
       timed_out = true;
       break;
@@ -692,12 +696,14 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
     }
   }
   if (timed_out && tid == 0) {
-    if (a.status != nullptr) atomicOr(a.status, LBM_STATUS_WAIT_TIMEOUT);
+    unsigned bits = LBM_STATUS_WAIT_TIMEOUT;
     // drain the copies still in flight into this CTA's shared memory
     for (long long kk = k; kk < k + p.stages; ++kk) {
       if (blockIdx.x + kk * G >= p.groups) break;
-      mbar_wait_bounded(&bars[kk % p.stages], (unsigned)((kk / p.stages) & 1), kTmaWaitPolls);
+      if (!mbar_wait_bounded(&bars[kk % p.stages], (unsigned)((kk / p.stages) & 1), kTmaWaitPolls))
+        bits |= LBM_STATUS_DRAIN_FAILED;
     }
+    if (a.status != nullptr) atomicOr(a.status, bits);
   }
 }
 
@@ -761,6 +767,7 @@ inline bool tma_plan(const Geom &g, int q, int bits, const void *fa, TmaPlan &p,
   p.stages = stages;
   p.row_bytes = (unsigned)row_bytes;
   p.groups = rows / R;
+  p.wait_polls = tma_wait_polls();
   smem = 128 + (size_t)stages * stage;
   const long long want = (long long)ctas * d.sms;
   grid = (unsigned)std::min<long long>(p.groups, want);

@@ -184,7 +184,10 @@ class LBMBase:
         buffers after an even number of steps, so it replays any number of
         times.  Captured on a side stream; nothing runs during capture."""
         lat = self.flow.lattice
-        key = (n, self.step > 100, lat.cur, getattr(self, "_fi", 0))
+        # the uniform forces are baked into the captured launches, so they
+        # are part of the key (a changed body force captures a new graph)
+        key = (n, self.step > 100, lat.cur, getattr(self, "_fi", 0), self.body_force,
+               tuple(self._g_old))
         cache = self.__dict__.setdefault("_graphs", {})
         g = cache.get(key)
         if g is None:

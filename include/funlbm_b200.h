@@ -41,6 +41,9 @@ extern "C" {
 #define LBM_STATUS_STENCIL_EMPTY 0x4u /* a marker's normalised weight sum != 1   */
                                       /* after step 100 (lbm/lbm3d.py:84-86)     */
 #define LBM_STATUS_WAIT_TIMEOUT 0x8u  /* a bounded device-side wait gave up      */
+#define LBM_STATUS_DRAIN_FAILED 0x10u /* after such a timeout, a kernel could not */
+                                      /* confirm that its own bulk copies ended:  */
+                                      /* treat the lattice buffers as lost        */
 
 /* ---- boundary codes: values of funlbm's BoundaryCondition (config/base.py:17-23) */
 #define LBM_BC_PERIODICAL 11000
@@ -246,11 +249,14 @@ int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, fl
  * the library: LBM_SPREAD_NOALLOC_MAX_NODES int32 (16 MiB), held on every GPU
  * that loads the library until the process exits.  Lattices with more nodes
  * are rejected with LBM_ERR_INVALID.  The call allocates nothing.  Its first
- * call on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls share the one array and each resets
- * the part it uses: calls whose work overlaps on the GPU race, so issue them
- * in order on one stream.  Arguments and results are those of ibm_spread
- * without `owner`. */
+ * call on a device looks up the array's device address, and its first
+ * reference-mode call (mode 0) on a device also sets the whole array to -1
+ * (every later call leaves it at -1 again); make those first calls before any
+ * stream capture.  The looked-up address belongs to the device's primary
+ * context: after cudaDeviceReset it is stale, so do not call this entry point
+ * again in that process.  All calls share the one array: calls whose work
+ * overlaps on the GPU race, so issue them in order on one stream.  Arguments
+ * and results are those of ibm_spread without `owner`. */
 #define LBM_SPREAD_NOALLOC_MAX_NODES (1 << 22)
 int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
                        uint8_t *chunks, void *stream);
@@ -259,6 +265,16 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
  * particle/coord.py:87-108): angle += cw; lx = R(angle) lagrange + cx, with the
  * rotation built in float64 from the rotation vector. */
 int rigid_update_markers(const lbm_particles *pt, void *stream);
+
+/* Test hook, no counterpart in the reference: poll limit of the consumer-side
+ * mbarrier waits of the row-staged step (lattices with step_nodes =
+ * LBM_STEP_ROWS) for the launches that follow, process-wide.  A negative
+ * value restores the default (2^24 polls, also the maximum); 0 makes every
+ * such wait give up before its first poll, so that the timeout path --
+ * LBM_STATUS_WAIT_TIMEOUT in the status word, the kernel's own bulk copies
+ * drained under the default limit, an orderly return -- can be exercised
+ * without a fault.  Populations of a step that timed out are incomplete. */
+void lbm_debug_set_wait_limit(int64_t polls);
 
 /* Thread-local message of the last failed call. */
 const char *lbm_last_error(void);

@@ -2,7 +2,9 @@
 
 Run in the build container (where the reference source is mounted):
 
-    python tests/golden/make_golden.py --reference /root/reference/src
+    python tests/golden/make_golden.py --reference <funlbm checkout>/src
+
+(or set FUNLBM_REFERENCE_SRC instead of --reference).
 
 The reference imports five packages that are absent here (funutil, funtable,
 funvtk, funtecplot, h5py); ``tests/golden/_stubs`` holds project-written
@@ -292,9 +294,12 @@ def make_markers():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference/src")
+    ap.add_argument("--reference", default=os.environ.get("FUNLBM_REFERENCE_SRC"),
+                    help="the funlbm source tree (its src/ directory)")
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("pass --reference or set FUNLBM_REFERENCE_SRC")
     _setup(args.reference)
     import torch
 

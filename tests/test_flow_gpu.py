@@ -440,3 +440,43 @@ def test_odd_rows_agree_bitwise(q, storage):
     ref = results[(1, 256)]
     for k, v in results.items():
         assert np.array_equal(v, ref), (k, np.abs(v - ref).max())
+
+
+def test_row_staged_wait_timeout_sets_status():
+    """The row-staged (TMA) step's consumer waits are bounded.  With the test
+    hook's limit at zero polls every such wait gives up at once: the kernel
+    sets LBM_STATUS_WAIT_TIMEOUT, drains its own bulk copies under the
+    default limit (no LBM_STATUS_DRAIN_FAILED) and returns; the context stays
+    usable and the default limit steps correctly again."""
+    from funlbm_b200 import _lib
+    from funlbm_b200.lattice import Lattice, make_force, tau_float32
+
+    q, shape, codes = 19, (9, 7, 16), [11000] * 6
+    f0 = smooth_f0(q, shape, 0.04, 21)
+    f0_soa = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda")
+    force = make_force((0, 0, 0), (0, 0, 0))
+    lib = _lib.load()
+    lat = Lattice(q, shape, codes, tau_float32(0.07), device="cuda")
+    lat.set_launch_shape(-1, 256)
+    lat.init(f0_soa)
+    lib.lbm_debug_set_wait_limit(0)
+    try:
+        lat.step(force)
+        torch.cuda.synchronize()
+    finally:
+        lib.lbm_debug_set_wait_limit(-1)
+    word = lat.read_status()
+    assert word & _lib.LBM_STATUS_WAIT_TIMEOUT
+    assert not word & _lib.LBM_STATUS_DRAIN_FAILED
+    results = []
+    for nodes in (-1, 1):
+        lat = Lattice(q, shape, codes, tau_float32(0.07), device="cuda")
+        lat.set_launch_shape(nodes, 256)
+        lat.init(f0_soa)
+        for _ in range(3):
+            lat.step(force)
+        assert lat.read_status() == 0
+        f = torch.empty(q * lat.n, device="cuda")
+        lat.observe(force, f=f)
+        results.append(to_np(f))
+    assert np.array_equal(results[0], results[1])

@@ -37,11 +37,14 @@ def _lattice(shape=SHAPE):
     return Lattice(19, shape, [1200] * 6, tau_float32(0.1), device="cuda", allocate=False)
 
 
-def _swarm():
+BODIES = ((3, [8.0, 9.5, 10.2]), (2.5, [11.3, 12.0, 12.7]), (4, [17.6, 10.4, 13.1]))
+
+
+def _swarm(bodies=BODIES):
     from funlbm_b200.particle import ParticleConfig, ParticleSwarm
 
     cfgs = [ParticleConfig().from_json({"type": "sphere", "r": r, "coord": {"center": c}})
-            for r, c in ((3, [8.0, 9.5, 10.2]), (2.5, [11.3, 12.0, 12.7]), (4, [17.6, 10.4, 13.1]))]
+            for r, c in bodies]
     sw = ParticleSwarm(cfgs, device="cuda")
     sw.init()
     sw.update()            # place the markers on the bodies
@@ -82,11 +85,46 @@ def test_noalloc_spread_matches_ibm_spread(mode):
         torch.cuda.synchronize()
         a, b = to_np(field_a), to_np(field_b)
         assert np.abs(a).max() > 0
-        # the tolerance of the spreading comparisons elsewhere in the suite
-        assert np.abs(b - a).max() <= 1e-4 * np.abs(a).max(), call
+        if mode == 0:
+            # last-writer-wins: one writer per node, no atomics -- the two
+            # entry points run the same deterministic kernels
+            assert np.array_equal(a, b), call
+        else:
+            # accumulation order of the atomics is not deterministic; the
+            # tolerance of the spreading comparisons elsewhere in the suite
+            assert np.abs(b - a).max() <= 1e-4 * np.abs(a).max(), call
         assert np.array_equal(to_np(chunks_a), to_np(chunks_b)), call
     # the caller-owned claim array is back to its resting value
     assert bool((owner == -1).all())
+
+
+def test_noalloc_spread_at_the_size_limit():
+    """A lattice of exactly LBM_SPREAD_NOALLOC_MAX_NODES nodes is accepted, and
+    markers next to its last nodes spread the same field as ibm_spread."""
+    from funlbm_b200 import _lib
+    from funlbm_b200._lib import ptr
+
+    lat = _lattice((256, 128, 128))
+    assert lat.n == _lib.SPREAD_NOALLOC_MAX_NODES
+    sw = _swarm(((3, [250.6, 122.3, 123.1]), (2.5, [5.2, 4.4, 3.9])))
+    n = lat.n
+    nch = (n + 31) // 32
+    field_a = torch.zeros(3 * n, device="cuda")
+    field_b = torch.zeros(3 * n, device="cuda")
+    chunks_a = torch.zeros(nch, dtype=torch.uint8, device="cuda")
+    chunks_b = torch.zeros(nch, dtype=torch.uint8, device="cuda")
+    owner = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    _forces(sw, 7)
+    st = ctypes.byref(sw.struct())
+    _lib.call("ibm_spread", ctypes.byref(lat.desc), st, 0, ptr(field_a), ptr(chunks_a), ptr(owner),
+              lat.stream())
+    _lib.call("ibm_spread_noalloc", ctypes.byref(lat.desc), st, 0, ptr(field_b), ptr(chunks_b),
+              lat.stream())
+    torch.cuda.synchronize()
+    a = to_np(field_a)
+    assert np.abs(a[3 * (n // 2):]).max() > 0          # the far body reached the upper half
+    assert np.array_equal(a, to_np(field_b))
+    assert np.array_equal(to_np(chunks_a), to_np(chunks_b))
 
 
 def test_noalloc_spread_rejects_large_lattice():
