@@ -12,9 +12,17 @@ so no flush is needed between steps).
 For N > 1 (torchrun) every rank advances its own independent lattice
 (replicas: the path has no exchange step); time = max over ranks.
 
-``--impl reference`` times the CPU restatement of the reference's step (the
-oracle, numpy) on the host cores on a bounded 64^3 sample of the same
-workload; under torchrun only rank 0 runs it.
+``--impl reference`` times the reference itself -- funlbm 1.2.0 installed
+unmodified in baseline/_ref, ``LBMD3.run_step`` through its public API -- on
+the host cores (torch threads = cpu_count, as funlbm's ``set_cpu`` sets them)
+on a bounded sample of the same workload (128^3 nodes, smaller when the run
+would not fit a few minutes), and adds the same reference path on the GPU
+(its torch code with the flow on ``cuda``) at the full size as
+``reference_gpu``; under torchrun only rank 0 runs it.  funlbm imports five
+helper packages that are not installable here; the project-written
+stand-ins in tests/golden/_stubs replace them (none of them is on the step
+path).  Without baseline/_ref the arm falls back to the oracle (numpy
+restatement, "port").
 """
 from __future__ import annotations
 
@@ -38,6 +46,9 @@ Q = 19
 TAU_MU = 1.0 / 30.0
 U0 = 0.05
 BYTES_PER_LU = {"fp32": 2 * Q * 4, "fp16s": 2 * Q * 2, "bf16s": 2 * Q * 2}
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+REF_STUBS = os.path.join(ROOT, "tests", "golden", "_stubs")
+FACE_NAMES = ("input", "output", "back", "forward", "bottom", "top")
 
 
 def metric_name(n, storage):
@@ -306,6 +317,153 @@ def oracle_workload(n):
     return lbm
 
 
+# ---------------------------------------------------------------------------
+# the reference itself (funlbm 1.2.0 from baseline/_ref)
+# ---------------------------------------------------------------------------
+def reference_available():
+    return os.path.isfile(os.path.join(REF_DIR, "funlbm", "__init__.py"))
+
+
+def import_reference():
+    """Put baseline/_ref (and the stand-ins of funlbm's five absent helper
+    packages) on the path.  Importing funlbm.lbm runs its set_cpu(), which sets
+    torch's intra-op threads to cpu_count."""
+    for p in (REF_STUBS, REF_DIR):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import funlbm.lbm  # noqa: F401
+
+
+def taylor_green_feq(n, param, device):
+    """f = feq(rho = 1, u_TG) as float32 [n, n, n, Q] with the reference's
+    equilibrium formula (flow/d3/base.py:152-158) and its own lattice
+    constants (`param`: e, w, cs of a funlbm flow), built on `device`."""
+    import torch
+
+    e, w, cs = param.e.to(device), param.w.to(device), param.cs.to(device)
+    k = 2 * np.pi / n
+    ax = torch.arange(n, device=device, dtype=torch.float32) * k
+    x, y, z = ax[:, None, None], ax[None, :, None], ax[None, None, :]
+    u = torch.stack(torch.broadcast_tensors(U0 * torch.sin(x) * torch.cos(y) * torch.cos(z),
+                                            -U0 * torch.cos(x) * torch.sin(y) * torch.cos(z),
+                                            torch.zeros_like(x)), -1)
+    tmp = (u @ e.t()) / cs ** 2
+    u2 = torch.linalg.norm(u, dim=-1, keepdim=True) ** 2 / cs ** 2 / 2
+    return (1 + tmp + tmp ** 2 / 2 - u2) * w
+
+
+def reference_workload(n, device, workdir):
+    """funlbm's own LBMD3 on an n^3 sample of the workload.  LBMBase takes its
+    device from Worker's default ("cpu") whatever the config says
+    (lbm/base.py:56-84, base/work.py:41-43), so the flow is created on
+    `device` with funlbm's create_flow and handed to LBMD3 (flow=...), the
+    reference's own injection point.  Initialisation as the reference's
+    LBMD3._init, with f replaced by the Taylor-Green equilibrium after
+    FlowD3.init."""
+    import_reference()
+    from funlbm.flow import create_flow
+    from funlbm.lbm import LBMD3, Config
+
+    cfg = Config().from_json({
+        "dt": 1, "dx": 1, "max_step": 10 ** 9,
+        "file": {"per_steps": 10 ** 9, "cache_dir": workdir},
+        "flow": {"size": [n - 1] * 3, "param_type": "D3Q%d" % Q, "param": {"mu": TAU_MU},
+                 "boundary": {k: {"code": "PERIODICAL"} for k in FACE_NAMES}}})
+    flow = create_flow(cfg.flow_config, device=device)
+    lbm = LBMD3(config=cfg, flow=flow)
+    lbm.flow.init()
+    lbm.flow.f = taylor_green_feq(n, lbm.flow.param, device)
+    lbm.flow.update_u_rou()
+    lbm.flow.cul_equ()
+    lbm.particle_swarm.init()
+    return lbm
+
+
+def reference_cpu(args, budget_s, max_steps=None):
+    """funlbm on the host cores: MLUPS on the largest sample (128^3 at most)
+    whose warm-up + timed steps fit `budget_s`.  Returns (line fields)."""
+    import torch
+
+    steps = args.steps if max_steps is None else min(args.steps, max_steps)
+    with tempfile.TemporaryDirectory() as tmp:
+        cwd = os.getcwd()
+        os.chdir(tmp)          # funlbm opens its logs relative to the cwd
+        try:
+            n = 128
+            lbm = reference_workload(n, "cpu", tmp)
+            t0 = time.perf_counter()
+            lbm.run_step(step=lbm.step)
+            t1 = time.perf_counter() - t0
+            want = (steps + args.warmup) * t1
+            if want > budget_s:
+                n = max(32, int(n * (budget_s / want) ** (1 / 3)) // 16 * 16)
+                del lbm
+                lbm = reference_workload(n, "cpu", tmp)
+                lbm.run_step(step=lbm.step)
+            for _ in range(args.warmup):
+                lbm.step += 1
+                lbm.run_step(step=lbm.step)
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                lbm.step += 1
+                lbm.run_step(step=lbm.step)
+            el = time.perf_counter() - t0
+        finally:
+            os.chdir(cwd)
+    cores = torch.get_num_threads()
+    return {"value": n ** 3 * steps / el / 1e6, "unit": "MLUPS", "cores": cores,
+            "kind": "reference", "n": n, "steps": steps, "seconds": el,
+            "sample": "funlbm 1.2.0 LBMD3.run_step (torch CPU, %d threads = cpu_count %d), %d^3 "
+                      "nodes of the periodic Taylor-Green workload, %d timed steps after %d "
+                      "warm-up, %.1f s" % (cores, os.cpu_count() or 0, n, steps, args.warmup, el)}
+
+
+def reference_gpu(args, max_steps=5):
+    """The reference's torch path with its flow on the GPU: CUDA-event MLUPS
+    at the workload's size (halved until its temporaries fit in memory)."""
+    import torch
+
+    if not torch.cuda.is_available():
+        return None
+    n = args.size
+    with tempfile.TemporaryDirectory() as tmp:
+        cwd = os.getcwd()
+        os.chdir(tmp)
+        try:
+            while n >= 64:
+                try:
+                    lbm = reference_workload(n, "cuda", tmp)
+                    for _ in range(max(1, min(args.warmup, 3))):
+                        lbm.run_step(step=lbm.step)
+                        lbm.step += 1
+                    steps = min(args.steps, max_steps)
+                    a = torch.cuda.Event(enable_timing=True)
+                    b = torch.cuda.Event(enable_timing=True)
+                    torch.cuda.synchronize()
+                    a.record()
+                    for _ in range(steps):
+                        lbm.run_step(step=lbm.step)
+                        lbm.step += 1
+                    b.record()
+                    torch.cuda.synchronize()
+                    ms = a.elapsed_time(b)
+                    peak = torch.cuda.max_memory_allocated() / 1e9
+                    del lbm
+                    torch.cuda.empty_cache()
+                    return {"value": n ** 3 * steps / (ms / 1e3) / 1e6, "unit": "MLUPS",
+                            "nodes_per_axis": n, "steps": steps, "ms_per_step": ms / steps,
+                            "peak_device_gb": peak,
+                            "path": "funlbm 1.2.0 LBMD3.run_step, flow created on cuda "
+                                    "(torch ATen kernels), CUDA events"}
+                except torch.cuda.OutOfMemoryError:
+                    lbm = None
+                    torch.cuda.empty_cache()
+                    n //= 2
+        finally:
+            os.chdir(cwd)
+    return None
+
+
 def host_threads():
     try:
         from threadpoolctl import threadpool_info
@@ -316,9 +474,15 @@ def host_threads():
 
 
 def cpu_baseline(args, seconds=12.0):
-    """The oracle (numpy restatement of the reference's step) on a bounded
-    sample: a cpu_size^3 lattice of the same workload, as many steps as fit
-    in `seconds`."""
+    """The reference's CPU path (funlbm from baseline/_ref) on a bounded sample
+    of the workload, about `seconds` of CPU work; without baseline/_ref the
+    oracle (numpy restatement of the reference's step) on a cpu_size^3
+    lattice, as many steps as fit in `seconds`."""
+    if reference_available():
+        res = reference_cpu(args, seconds, max_steps=10)
+        for k in ("n", "steps", "seconds"):
+            res.pop(k, None)
+        return res
     n = args.cpu_size
     lbm = oracle_workload(n)
     lbm.run(1)
@@ -575,9 +739,33 @@ def profiled_traffic(args):
 
 
 def main_reference(args, world, rank):
-    """CPU arm: the oracle port of the reference step, each step one step of a
-    cpu_size^3 sample of the workload, on the host cores."""
+    """Reference arm: funlbm itself on the host cores (each step one run_step
+    of a bounded sample of the workload), plus the same path on the GPU as
+    reference_gpu; the oracle port when baseline/_ref is absent."""
     if rank != 0:
+        return
+    if reference_available():
+        cpu = reference_cpu(args, budget_s=150.0)
+        value, n = cpu.pop("value"), cpu.pop("n")
+        steps, el = cpu.pop("steps"), cpu.pop("seconds")
+        line = {
+            "impl": "reference", "metric": metric_name(args.size, "fp32"), "value": value,
+            "unit": "MLUPS", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / max(steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (Taylor-Green vortex initial field, u0=0.05)",
+            "config": {"workload": "D3Q19 fp32, all faces periodic, tau 0.6, Taylor-Green u0=0.05;"
+                                   " CPU sample %d^3 of the %d^3 workload" % (n, args.size),
+                       "sample_nodes": n ** 3},
+            "cpu_baseline": dict(cpu, value=value, unit="MLUPS"),
+            "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        try:
+            line["reference_gpu"] = reference_gpu(args)
+        except Exception as exc:        # the CPU figure stands on its own
+            line["reference_gpu"] = {"unavailable": "%s: %s" % (type(exc).__name__, exc)}
+        print(json.dumps(line), flush=True)
         return
     n = args.cpu_size
     lbm = oracle_workload(n)

@@ -23,7 +23,7 @@ LBM_STATUS_STENCIL_EMPTY = 0x4
 LBM_STATUS_WAIT_TIMEOUT = 0x8
 LBM_STATUS_DRAIN_FAILED = 0x10
 
-STORAGE = {"fp32": 0, "fp16s": 1, "bf16s": 2}
+STORAGE = {"fp32": 0, "fp16s": 1, "bf16s": 2, "fp64": 3}
 SPREAD_NOALLOC_MAX_NODES = 1 << 22
 RIGID_WALL = 1
 RIGID_UPDATE = 2
@@ -85,6 +85,7 @@ class LbmParticles(ctypes.Structure):
         ("mass", ctypes.c_void_p),
         ("inertia", ctypes.c_void_p),
         ("rou", ctypes.c_void_p),
+        ("fp64", ctypes.c_int32),
     ]
 
 

@@ -42,7 +42,7 @@ def _nvcc():
 
 
 INSTANCED = "lbm_step_inst.cu"   # compiled once per (velocity set, storage)
-INSTANCES = [(q, st) for q in (13, 15, 19, 27) for st in (0, 1, 2)]
+INSTANCES = [(q, st) for q in (13, 15, 19, 27) for st in (0, 1, 2, 3)]
 
 
 def _sources():

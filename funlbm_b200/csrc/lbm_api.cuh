@@ -18,6 +18,10 @@ Geom make_geom(const lbm_lattice *lat);
 // pull-source / face-source / destination plane pointers of a lattice step
 void fill_step_planes(const Geom &g, int q, int storage, const void *fa, void *fb, StepPlanes &p);
 bool any_face(const lbm_lattice *lat, int code);
+// bits of one stored population
+inline int storage_bits(int storage) {
+  return storage == LBM_STORAGE_FP32 ? 32 : storage == LBM_STORAGE_FP64 ? 64 : 16;
+}
 // default poll limit of every bounded mbarrier wait in the TMA-staged step
 constexpr unsigned kTmaWaitPollsDefault = 1u << 24;
 // poll limit of its consumer waits for the next launches (lbm_debug_set_wait_limit)

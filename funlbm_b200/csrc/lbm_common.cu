@@ -59,7 +59,7 @@ int check_lattice(const lbm_lattice *lat) {
     set_error("relaxation time tau=%g must exceed 0.5", (double)lat->tau);
     return LBM_ERR_INVALID;
   }
-  if (lat->storage < LBM_STORAGE_FP32 || lat->storage > LBM_STORAGE_BF16S) {
+  if (lat->storage < LBM_STORAGE_FP32 || lat->storage > LBM_STORAGE_FP64) {
     set_error("unknown population storage %d", lat->storage);
     return LBM_ERR_INVALID;
   }
@@ -112,6 +112,15 @@ Geom make_geom(const lbm_lattice *lat) {
   g.force_c = 1.0f - 1.0f / (2.0f * lat->tau);
   g.re_mu = lat->re_mu;
   g.neq_profile = lat->neq_profile;
+  const double tau = (double)lat->tau;
+  const double cs = std::sqrt(1.0 / 3.0);
+  const double cs2 = cs * cs;
+  g.inv_tau_d = 1.0 / tau;
+  g.inv_cs2_d = 1.0 / cs2;
+  g.inv_cs4_d = 1.0 / (cs2 * cs2);
+  g.force_c_d = 1.0 - 1.0 / (2.0 * tau);
+  for (int i = 0; i < LBM_NFACES; ++i)
+    for (int k = 0; k < 3; ++k) g.uw_d[i][k] = (double)lat->face_uw[i][k];
   return g;
 }
 
@@ -139,7 +148,7 @@ static void fill_planes_q(const Geom &g, const void *fa, void *fb, int elem, Ste
 
 void fill_step_planes(const Geom &g, int q, int storage, const void *fa, void *fb,
                              StepPlanes &p) {
-  const int elem = storage == LBM_STORAGE_FP32 ? 4 : 2;
+  const int elem = storage_bits(storage) / 8;
   switch (q) {
     case 13: fill_planes_q<13>(g, fa, fb, elem, p); break;
     case 15: fill_planes_q<15>(g, fa, fb, elem, p); break;

@@ -27,27 +27,30 @@ static int run_step(const StepArgs &a, int q, int storage, bool force, int nodes
 // then two collisions with those same moments (LBMD3._init's cul_equ and
 // step 1's cul_equ, which the reference runs before refreshing the moments).
 // ---------------------------------------------------------------------------
+// f0 and face_rho hold the storage's arithmetic type (float64 for FP64).
 template <int Q, int S>
 __global__ void __launch_bounds__(kThreads)
-    k_init(const Geom g, const NodeDecomp dec, const float *f0, void *fa_, float *face_rho) {
+    k_init(const Geom g, const NodeDecomp dec, const void *f0_, void *fa_, void *face_rho_) {
   using V = VSet<Q>;
   using St = Storage<S>;
+  using R = typename St::R;
   const unsigned idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= (unsigned)g.n) return;
   int x, y, z;
   dec(idx, x, y, z);
   const bool face = on_any_face(g, x, y, z);
-  float f[Q];
+  const R *f0 = static_cast<const R *>(f0_);
+  R f[Q];
 #pragma unroll
-  for (int i = 0; i < Q; ++i) f[i] = f0 ? f0[(long long)i * g.n + idx] : V::w(i);
-  float rho, ux, uy, uz;
-  moments<Q>(f, 0.f, 0.f, 0.f, face, rho, ux, uy, uz);
+  for (int i = 0; i < Q; ++i) f[i] = f0 ? f0[(long long)i * g.n + idx] : V::template wr<R>(i);
+  R rho, ux, uy, uz;
+  moments<Q>(f, R(0), R(0), R(0), face, rho, ux, uy, uz);
   collide<Q>(f, g, rho, ux, uy, uz);
   collide<Q>(f, g, rho, ux, uy, uz);
-  if (face && face_rho != nullptr) write_face_rho<Q>(g, face_rho, x, y, z, rho);
+  if (face && face_rho_ != nullptr) write_face_rho<Q>(g, static_cast<R *>(face_rho_), x, y, z, rho);
   typename St::T *fa = static_cast<typename St::T *>(fa_);
 #pragma unroll
-  for (int i = 0; i < Q; ++i) St::store(fa + (long long)i * g.n + idx, f[i], V::w(i));
+  for (int i = 0; i < Q; ++i) St::store(fa + (long long)i * g.n + idx, f[i], V::template wr<R>(i));
 }
 
 // ---------------------------------------------------------------------------
@@ -215,7 +218,7 @@ int dispatch_q(int q, A &&...args) {
 
 template <int Q>
 struct RunInit {
-  static int run(const Geom &g, const float *f0, void *fa, float *face_rho, int storage,
+  static int run(const Geom &g, const void *f0, void *fa, void *face_rho, int storage,
                  cudaStream_t s) {
     const unsigned nb = blocks_for(g.n, kThreads);
     const NodeDecomp dec = make_decomp(g);
@@ -225,6 +228,9 @@ struct RunInit {
         break;
       case LBM_STORAGE_FP16S:
         k_init<Q, LBM_STORAGE_FP16S><<<nb, kThreads, 0, s>>>(g, dec, f0, fa, face_rho);
+        break;
+      case LBM_STORAGE_FP64:
+        k_init<Q, LBM_STORAGE_FP64><<<nb, kThreads, 0, s>>>(g, dec, f0, fa, face_rho);
         break;
       default:
         k_init<Q, LBM_STORAGE_BF16S><<<nb, kThreads, 0, s>>>(g, dec, f0, fa, face_rho);
@@ -346,7 +352,8 @@ int lbm_flow_init(const lbm_lattice *lat, const float *f0, void *fa, float *face
     return LBM_ERR_INVALID;
   }
   const Geom g = make_geom(lat);
-  return dispatch_q<RunInit>(lat->q, g, f0, fa, face_rho, lat->storage, (cudaStream_t)stream);
+  return dispatch_q<RunInit>(lat->q, g, static_cast<const void *>(f0), fa,
+                             static_cast<void *>(face_rho), lat->storage, (cudaStream_t)stream);
 }
 
 int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_force *force,
@@ -357,7 +364,7 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
   int rc = build_step_args(lat, fa, fb, force, face_rho_in, face_rho_out, obs, status, a,
                            use_force, "lbm_flow_step");
   if (rc) return rc;
-  const int bits = lat->storage == LBM_STORAGE_FP32 ? 32 : 16;
+  const int bits = storage_bits(lat->storage);
   if (lat->step_nodes != 0 && lat->step_nodes != LBM_STEP_ROWS &&
       !step_shape_legal(lat->step_nodes, lat->nz, bits)) {
     set_error("lbm_flow_step: %d nodes per thread does not fit rows of %d nodes (%d-bit storage)",
@@ -390,7 +397,7 @@ int lbm_batch_pack(const lbm_lattice *lat, const void *fa, void *fb, const lbm_f
   int rc = build_step_args(lat, fa, fb, force, face_rho_in, face_rho_out, nullptr, status, a,
                            use_force, "lbm_batch_pack");
   if (rc) return rc;
-  const int bits = lat->storage == LBM_STORAGE_FP32 ? 32 : 16;
+  const int bits = storage_bits(lat->storage);
   if (nodes != 1 && !((nodes == 2 || nodes == 4) && step_shape_ok(nodes, lat->nz, bits))) {
     set_error("lbm_batch_pack: nodes per thread must be 1, or 2 / 4 for rows of a multiple of "
               "that many nodes (at least twice as many)");

@@ -19,28 +19,32 @@ constexpr int kRigidThreads = 256;
 // part of a stencil).  Computed in float32 like the reference.
 // lo is also capped at size (the box is then empty) so that markers far
 // outside the domain (or non-finite) never produce an out-of-range index.
-__device__ __forceinline__ void box_axis(float l, int size, int &lo, int &hi) {
-  float rl = floorf(l) - 1.f;
-  rl = fmaxf(rl, 0.f);
-  float rr = fminf(rl + 4.f, (float)size);
-  rl = fminf(rl, (float)size);
-  rr = fmaxf(rr, 0.f);
+// R is the arithmetic type: float, or double for FP64 lattices.
+template <typename R>
+__device__ __forceinline__ void box_axis(R l, int size, int &lo, int &hi) {
+  R rl = floor(l) - R(1);
+  rl = fmax(rl, R(0));
+  R rr = fmin(rl + R(4), (R)size);
+  rl = fmin(rl, (R)size);
+  rr = fmax(rr, R(0));
   lo = (int)rl;
   hi = (int)rr;
 }
 
 // 4-point cosine delta of lbm/lbm3d.py:46-64, one axis:
 // (1 + cos(|r pi / 2|)) / 4, and the |r| <= 2 test of the mask.
-__device__ __forceinline__ float delta_axis(float r, bool &inside) {
-  inside = inside && (fabsf(r) <= 2.f);
-  const float arg = fabsf(r * 3.14159265358979323846f / 2.f);
-  return (1.f + cosf(arg)) / 4.f;
+template <typename R>
+__device__ __forceinline__ R delta_axis(R r, bool &inside) {
+  inside = inside && (fabs(r) <= R(2));
+  const R arg = fabs(r * R(3.14159265358979323846) / R(2));
+  return (R(1) + cos(arg)) / R(4);
 }
 
 // Unnormalised weight of stencil slot j of a marker at `l`; false if the slot
 // is outside the (clamped) box.
-__device__ __forceinline__ bool stencil_slot(const Geom &g, const float l[3], int j, int &x, int &y,
-                                             int &z, float &w) {
+template <typename R>
+__device__ __forceinline__ bool stencil_slot(const Geom &g, const R l[3], int j, int &x, int &y,
+                                             int &z, R &w) {
   int lo[3], hi[3];
   box_axis(l[0], g.nx - 1, lo[0], hi[0]);
   box_axis(l[1], g.ny - 1, lo[1], hi[1]);
@@ -50,16 +54,16 @@ __device__ __forceinline__ bool stencil_slot(const Geom &g, const float l[3], in
   z = lo[2] + (j & 3);
   if (x >= hi[0] || y >= hi[1] || z >= hi[2]) return false;
   bool in = true;
-  const float wx = delta_axis((float)x - l[0], in);
-  const float wy = delta_axis((float)y - l[1], in);
-  const float wz = delta_axis((float)z - l[2], in);
-  w = in ? (wx * wy) * wz : 0.f;
+  const R wx = delta_axis((R)x - l[0], in);
+  const R wy = delta_axis((R)y - l[1], in);
+  const R wz = delta_axis((R)z - l[2], in);
+  w = in ? (wx * wy) * wz : R(0);
   return true;
 }
 
 // Sum over the 64 stencil threads of one marker (two warps) via shared memory.
-template <int N>
-__device__ __forceinline__ void stencil_sum(float (&v)[N], float (*sh)[kMarkersPerBlock * 2], int slot,
+template <int N, typename R>
+__device__ __forceinline__ void stencil_sum(R (&v)[N], R (*sh)[kMarkersPerBlock * 2], int slot,
                                             int mk) {
 #pragma unroll
   for (int k = 0; k < N; ++k)
@@ -74,16 +78,48 @@ __device__ __forceinline__ void stencil_sum(float (&v)[N], float (*sh)[kMarkersP
   for (int k = 0; k < N; ++k) v[k] = sh[k][mk * 2] + sh[k][mk * 2 + 1];
 }
 
+// The particle arrays of an lbm_particles in the arithmetic type R (its
+// `float *` members hold float64 when the struct's fp64 flag is set).
+template <typename R>
+struct PView {
+  const int32_t *offset, *owner;
+  const R *lagrange, *lm, *mass, *inertia, *rou;
+  R *lx, *lu, *lF, *lrou, *cx, *cu, *cw, *cF, *cT, *angle;
+};
+
+template <typename R>
+__device__ __forceinline__ PView<R> pview(const lbm_particles &p) {
+  PView<R> v;
+  v.offset = p.marker_offset;
+  v.owner = p.marker_owner;
+  v.lagrange = reinterpret_cast<const R *>(p.lagrange);
+  v.lm = reinterpret_cast<const R *>(p.lm);
+  v.mass = reinterpret_cast<const R *>(p.mass);
+  v.inertia = reinterpret_cast<const R *>(p.inertia);
+  v.rou = reinterpret_cast<const R *>(p.rou);
+  v.lx = reinterpret_cast<R *>(p.lx);
+  v.lu = reinterpret_cast<R *>(p.lu);
+  v.lF = reinterpret_cast<R *>(p.lF);
+  v.lrou = reinterpret_cast<R *>(p.lrou);
+  v.cx = reinterpret_cast<R *>(p.cx);
+  v.cu = reinterpret_cast<R *>(p.cu);
+  v.cw = reinterpret_cast<R *>(p.cw);
+  v.cF = reinterpret_cast<R *>(p.cF);
+  v.cT = reinterpret_cast<R *>(p.cT);
+  v.angle = reinterpret_cast<R *>(p.angle);
+  return v;
+}
+
 // ---------------------------------------------------------------------------
 // Interpolation: thread = (marker, stencil slot).
 // ---------------------------------------------------------------------------
 struct InterpArgs {
   Geom g;
   const void *fa;
-  const float *u_field, *rho_field;
+  const void *u_field, *rho_field;   // arithmetic type of the lattice
   float go[3];
-  const float *fol_old;
-  const float *face_rho_in;
+  const void *fol_old;
+  const void *face_rho_in;
   lbm_particles p;
   float dt;
   int step;
@@ -93,40 +129,46 @@ struct InterpArgs {
 
 template <int Q, int S>
 __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
-  __shared__ float sh[3][kMarkersPerBlock * 2];
+  using R = typename Storage<S>::R;
+  __shared__ R sh[3][kMarkersPerBlock * 2];
+  const PView<R> P = pview<R>(a.p);
   const int mk = threadIdx.x / kStencil, slot = threadIdx.x % kStencil;
   const int m = blockIdx.x * kMarkersPerBlock + mk;
   const bool live = m < a.p.n_markers;
-  float acc[3] = {0.f, 0.f, 0.f};  // sum w, sum w (ux+uy+uz), sum w rho
-  float l[3] = {0.f, 0.f, 0.f};
+  R acc[3] = {R(0), R(0), R(0)};  // sum w, sum w (ux+uy+uz), sum w rho
+  R l[3] = {R(0), R(0), R(0)};
   if (live) {
-    l[0] = a.p.lx[3 * m];
-    l[1] = a.p.lx[3 * m + 1];
-    l[2] = a.p.lx[3 * m + 2];
+    l[0] = P.lx[3 * m];
+    l[1] = P.lx[3 * m + 1];
+    l[2] = P.lx[3 * m + 2];
     int x, y, z;
-    float w;
+    R w;
     if (stencil_slot(a.g, l, slot, x, y, z, w)) {
       const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
-      float rho, ux, uy, uz;
+      R rho, ux, uy, uz;
       if (a.fa != nullptr) {
         const typename Storage<S>::T *fa = static_cast<const typename Storage<S>::T *>(a.fa);
-        float f[Q];
+        const R *face_rho = static_cast<const R *>(a.face_rho_in);
+        R f[Q];
         if (x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1)
-          pull_row_node<Q, S, false>(a.planes, a.g, a.face_rho_in, (unsigned)idx, x, y, z, f);
+          pull_row_node<Q, S, false>(a.planes, a.g, face_rho, (unsigned)idx, x, y, z, f);
         else
-          pull_general<Q, S>(fa, a.g, x, y, z, a.face_rho_in, f);
-        float fx = a.go[0], fy = a.go[1], fz = a.go[2];
+          pull_general<Q, S>(fa, a.g, x, y, z, face_rho, f);
+        R fx = a.go[0], fy = a.go[1], fz = a.go[2];
         if (a.fol_old != nullptr) {
-          fx += a.fol_old[3 * idx];
-          fy += a.fol_old[3 * idx + 1];
-          fz += a.fol_old[3 * idx + 2];
+          const R *fol = static_cast<const R *>(a.fol_old);
+          fx += fol[3 * idx];
+          fy += fol[3 * idx + 1];
+          fz += fol[3 * idx + 2];
         }
         moments<Q>(f, fx, fy, fz, on_any_face(a.g, x, y, z), rho, ux, uy, uz);
       } else {
-        rho = a.rho_field[idx];
-        ux = a.u_field[3 * idx];
-        uy = a.u_field[3 * idx + 1];
-        uz = a.u_field[3 * idx + 2];
+        const R *rf = static_cast<const R *>(a.rho_field);
+        const R *uf = static_cast<const R *>(a.u_field);
+        rho = rf[idx];
+        ux = uf[3 * idx];
+        uy = uf[3 * idx + 1];
+        uz = uf[3 * idx + 2];
       }
       acc[0] = w;
       acc[1] = w * ((ux + uy) + uz);
@@ -135,22 +177,21 @@ __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
   }
   stencil_sum<3>(acc, sh, slot, mk);
   if (!live || slot != 0) return;
-  const float W = acc[0];
-  const float lus = W > 0.f ? acc[1] / W : acc[1];
-  const float lrho = W > 0.f ? acc[2] / W : acc[2];
-  if (!(W > 0.f) && a.step > 100 && a.status != nullptr) atomicOr(a.status, LBM_STATUS_STENCIL_EMPTY);
-  const int pi = a.p.marker_owner[m];
-  const float rx = l[0] - a.p.cx[3 * pi], ry = l[1] - a.p.cx[3 * pi + 1],
-              rz = l[2] - a.p.cx[3 * pi + 2];
-  const float wx = a.p.cw[3 * pi], wy = a.p.cw[3 * pi + 1], wz = a.p.cw[3 * pi + 2];
-  const float v[3] = {a.p.cu[3 * pi] + (wy * rz - wz * ry), a.p.cu[3 * pi + 1] + (wz * rx - wx * rz),
-                      a.p.cu[3 * pi + 2] + (wx * ry - wy * rx)};
+  const R W = acc[0];
+  const R lus = W > R(0) ? acc[1] / W : acc[1];
+  const R lrho = W > R(0) ? acc[2] / W : acc[2];
+  if (!(W > R(0)) && a.step > 100 && a.status != nullptr) atomicOr(a.status, LBM_STATUS_STENCIL_EMPTY);
+  const int pi = P.owner[m];
+  const R rx = l[0] - P.cx[3 * pi], ry = l[1] - P.cx[3 * pi + 1], rz = l[2] - P.cx[3 * pi + 2];
+  const R wx = P.cw[3 * pi], wy = P.cw[3 * pi + 1], wz = P.cw[3 * pi + 2];
+  const R v[3] = {P.cu[3 * pi] + (wy * rz - wz * ry), P.cu[3 * pi + 1] + (wz * rx - wx * rz),
+                  P.cu[3 * pi + 2] + (wx * ry - wy * rx)};
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    a.p.lu[3 * m + k] = v[k];
-    a.p.lF[3 * m + k] = (2.f * lrho) * (v[k] - lus) / a.dt;
+    P.lu[3 * m + k] = v[k];
+    P.lF[3 * m + k] = (R(2) * lrho) * (v[k] - lus) / (R)a.dt;
   }
-  a.p.lrou[m] = lrho;
+  P.lrou[m] = lrho;
 }
 
 // ---------------------------------------------------------------------------
@@ -164,7 +205,8 @@ struct RigidArgs {
   float dt, dx, gl, rouf;
 };
 
-__device__ __forceinline__ void argext_merge(float &v, int &i, float v2, int i2, bool want_min) {
+template <typename R>
+__device__ __forceinline__ void argext_merge(R &v, int &i, R v2, int i2, bool want_min) {
   const bool better = want_min ? (v2 < v || (v2 == v && i2 < i)) : (v2 > v || (v2 == v && i2 < i));
   if (better) {
     v = v2;
@@ -172,34 +214,36 @@ __device__ __forceinline__ void argext_merge(float &v, int &i, float v2, int i2,
   }
 }
 
+template <typename R>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
+  const PView<R> P = pview<R>(a.p);
   const int pi = blockIdx.x;
-  const int m0 = a.p.marker_offset[pi], m1 = a.p.marker_offset[pi + 1];
-  __shared__ float s_v[6][kRigidThreads / 32];
+  const int m0 = P.offset[pi], m1 = P.offset[pi + 1];
+  __shared__ R s_v[6][kRigidThreads / 32];
   __shared__ int s_i[6][kRigidThreads / 32];
   __shared__ int s_ext[6];
   __shared__ double s_sum[3][kRigidThreads / 32];
-  __shared__ float s_cx[3];
+  __shared__ R s_cx[3];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 
   // -- extreme markers: argmin x,y,z then argmax x,y,z (first index on ties)
-  float v[6];
+  R v[6];
   int id[6];
   for (int k = 0; k < 3; ++k) {
-    v[k] = INFINITY;
-    v[k + 3] = -INFINITY;
+    v[k] = R(INFINITY);
+    v[k + 3] = -R(INFINITY);
     id[k] = id[k + 3] = 0x7fffffff;
   }
   for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
     for (int k = 0; k < 3; ++k) {
-      const float c = a.p.lx[3 * m + k];
+      const R c = P.lx[3 * m + k];
       argext_merge(v[k], id[k], c, m, true);
       argext_merge(v[k + 3], id[k + 3], c, m, false);
     }
   }
   for (int k = 0; k < 6; ++k) {
     for (int o = 16; o > 0; o >>= 1) {
-      const float v2 = __shfl_xor_sync(0xffffffffu, v[k], o);
+      const R v2 = __shfl_xor_sync(0xffffffffu, v[k], o);
       const int i2 = __shfl_xor_sync(0xffffffffu, id[k], o);
       argext_merge(v[k], id[k], v2, i2, k < 3);
     }
@@ -211,7 +255,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
   __syncthreads();
   if (threadIdx.x == 0 && (a.what & RIGID_WALL)) {
     for (int k = 0; k < 6; ++k) {
-      float bv = s_v[k][0];
+      R bv = s_v[k][0];
       int bi = s_i[k][0];
       for (int w = 1; w < kRigidThreads / 32; ++w) argext_merge(bv, bi, s_v[k][w], s_i[k][w], k < 3);
       s_ext[k] = bi;
@@ -221,23 +265,23 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
     if (valid) {  // (non-finite positions leave no extreme marker: no spring)
       // spring force k0 (1 - |x - wall| / (2 dx)), clamped at 0; the indexed
       // += of the reference reads all six old values and the last write wins
-      const float k0 = 300.f;
-      float d[6], dmax = 0.f;
+      const R k0 = R(300);
+      R d[6], dmax = R(0);
       for (int k = 0; k < 6; ++k) {
-        const float c = a.p.lx[3 * s_ext[k] + (k % 3)];
-        const float b = k < 3 ? 0.f : a.size[k - 3];
-        d[k] = fmaxf(k0 * (1.f - fabsf(c - b) / (2.f * a.dx)), 0.f);
-        dmax = fmaxf(dmax, d[k]);
+        const R c = P.lx[3 * s_ext[k] + (k % 3)];
+        const R b = k < 3 ? R(0) : (R)a.size[k - 3];
+        d[k] = fmax(k0 * (R(1) - fabs(c - b) / (R(2) * (R)a.dx)), R(0));
+        dmax = fmax(dmax, d[k]);
       }
-      if (dmax != 0.f) {
-        float nv[6][3];
+      if (dmax != R(0)) {
+        R nv[6][3];
         for (int k = 0; k < 6; ++k)
           for (int c = 0; c < 3; ++c) {
-            const float nrm = (c == k % 3) ? (k < 3 ? 1.f : -1.f) : 0.f;
-            nv[k][c] = a.p.lF[3 * s_ext[k] + c] + nrm * d[k];
+            const R nrm = (c == k % 3) ? (k < 3 ? R(1) : R(-1)) : R(0);
+            nv[k][c] = P.lF[3 * s_ext[k] + c] + nrm * d[k];
           }
         for (int k = 0; k < 6; ++k)
-          for (int c = 0; c < 3; ++c) a.p.lF[3 * s_ext[k] + c] = nv[k][c];
+          for (int c = 0; c < 3; ++c) P.lF[3 * s_ext[k] + c] = nv[k][c];
       }
     }
   }
@@ -247,8 +291,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
   // -- cF = sum(-lF lm) + (1 - rho_p / rho_f) mass [gl, 0, 0]   (float64 sums)
   double sf[3] = {0.0, 0.0, 0.0};
   for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double lm = a.p.lm[m];
-    for (int k = 0; k < 3; ++k) sf[k] += -(double)a.p.lF[3 * m + k] * lm;
+    const double lm = P.lm[m];
+    for (int k = 0; k < 3; ++k) sf[k] += -(double)P.lF[3 * m + k] * lm;
   }
   for (int k = 0; k < 3; ++k) {
     for (int o = 16; o > 0; o >>= 1) sf[k] += __shfl_xor_sync(0xffffffffu, sf[k], o);
@@ -256,17 +300,17 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const float mass = a.p.mass[pi];
-    const float buoy = (float)(1.0 - (double)a.p.rou[pi] / (double)a.rouf) * mass;
+    const R mass = P.mass[pi];
+    const R buoy = (R)(1.0 - (double)P.rou[pi] / (double)a.rouf) * mass;
     for (int k = 0; k < 3; ++k) {
       double t = 0.0;
       for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
-      const float cf = (float)t + (k == 0 ? buoy * a.gl : 0.f);
-      a.p.cF[3 * pi + k] = cf;
-      const float cu = a.p.cu[3 * pi + k] + cf / mass * a.dt;
-      a.p.cu[3 * pi + k] = cu;
-      const float cx = a.p.cx[3 * pi + k] + cu * a.dt;
-      a.p.cx[3 * pi + k] = cx;
+      const R cf = (R)t + (k == 0 ? buoy * (R)a.gl : R(0));
+      P.cF[3 * pi + k] = cf;
+      const R cu = P.cu[3 * pi + k] + cf / mass * (R)a.dt;
+      P.cu[3 * pi + k] = cu;
+      const R cx = P.cx[3 * pi + k] + cu * (R)a.dt;
+      P.cx[3 * pi + k] = cx;
       s_cx[k] = cx;
     }
   }
@@ -275,11 +319,11 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
   // -- cT = -sum((lx - cx) x lF lm)  with the new cx   (float64 sums)
   double st[3] = {0.0, 0.0, 0.0};
   for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double rx = (double)(a.p.lx[3 * m] - s_cx[0]);
-    const double ry = (double)(a.p.lx[3 * m + 1] - s_cx[1]);
-    const double rz = (double)(a.p.lx[3 * m + 2] - s_cx[2]);
-    const double fx = a.p.lF[3 * m], fy = a.p.lF[3 * m + 1], fz = a.p.lF[3 * m + 2];
-    const double lm = a.p.lm[m];
+    const double rx = (double)(P.lx[3 * m] - s_cx[0]);
+    const double ry = (double)(P.lx[3 * m + 1] - s_cx[1]);
+    const double rz = (double)(P.lx[3 * m + 2] - s_cx[2]);
+    const double fx = P.lF[3 * m], fy = P.lF[3 * m + 1], fz = P.lF[3 * m + 2];
+    const double lm = P.lm[m];
     st[0] += (ry * fz - rz * fy) * lm;
     st[1] += (rz * fx - rx * fz) * lm;
     st[2] += (rx * fy - ry * fx) * lm;
@@ -294,9 +338,9 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
     for (int k = 0; k < 3; ++k) {
       double t = 0.0;
       for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
-      const float ct = -(float)t;
-      a.p.cT[3 * pi + k] = ct;
-      a.p.cw[3 * pi + k] = a.p.cw[3 * pi + k] + 0.1f * ct * a.dt / a.p.inertia[3 * pi + k];
+      const R ct = -(R)t;
+      P.cT[3 * pi + k] = ct;
+      P.cw[3 * pi + k] = P.cw[3 * pi + k] + R(0.1) * ct * (R)a.dt / P.inertia[3 * pi + k];
     }
   }
 }
@@ -308,7 +352,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
 // the flag of one chunk; the warp then clears its flagged chunks together
 // (3 floats per lane per chunk), so a mostly flagged small lattice costs no
 // more than a sparse large one.
-__global__ void k_spread_clear(long long n, float *field, uint8_t *chunks) {
+template <typename R>
+__global__ void k_spread_clear(long long n, R *field, uint8_t *chunks) {
   const long long chunk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nchunks = (n + 31) >> 5;
   const int lane = threadIdx.x & 31;
@@ -320,7 +365,7 @@ __global__ void k_spread_clear(long long n, float *field, uint8_t *chunks) {
     todo &= todo - 1;
     const long long first = (base + j) * 32;
     const long long count = 3 * ((first + 32 < n ? first + 32 : n) - first);
-    for (long long k = lane; k < count; k += 32) field[3 * first + k] = 0.f;
+    for (long long k = lane; k < count; k += 32) field[3 * first + k] = R(0);
   }
   if (mine) chunks[chunk] = 0;
 }
@@ -328,7 +373,7 @@ __global__ void k_spread_clear(long long n, float *field, uint8_t *chunks) {
 struct SpreadArgs {
   Geom g;
   lbm_particles p;
-  float *field;
+  void *field;   // [n][3] in the arithmetic type of the particles
   uint8_t *chunks;
   int *owner;
 };
@@ -337,20 +382,22 @@ struct SpreadArgs {
 // pass 1: the owning marker writes w lF lm (reference mode)
 // pass 2: release the claims
 // pass 3: accumulate w lF lm (accumulate mode; flags set as in pass 0)
-template <int PASS>
+template <int PASS, typename R>
 __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
-  __shared__ float sh[1][kMarkersPerBlock * 2];
+  __shared__ R sh[1][kMarkersPerBlock * 2];
+  const PView<R> P = pview<R>(a.p);
+  R *field = static_cast<R *>(a.field);
   const int mk = threadIdx.x / kStencil, slot = threadIdx.x % kStencil;
   const int m = blockIdx.x * kMarkersPerBlock + mk;
   const bool live = m < a.p.n_markers;
-  float l[3] = {0.f, 0.f, 0.f};
+  R l[3] = {R(0), R(0), R(0)};
   int x = 0, y = 0, z = 0;
-  float w = 0.f;
+  R w = R(0);
   bool in_box = false;
   if (live) {
-    l[0] = a.p.lx[3 * m];
-    l[1] = a.p.lx[3 * m + 1];
-    l[2] = a.p.lx[3 * m + 2];
+    l[0] = P.lx[3 * m];
+    l[1] = P.lx[3 * m + 1];
+    l[2] = P.lx[3 * m + 2];
     in_box = stencil_slot(a.g, l, slot, x, y, z, w);
   }
   const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
@@ -365,17 +412,17 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
     return;
   }
   // passes 1 and 3 need the normalised weight: sum over the marker's stencil
-  float W[1] = {in_box ? w : 0.f};
+  R W[1] = {in_box ? w : R(0)};
   stencil_sum<1>(W, sh, slot, mk);
   if (!in_box) return;
-  const float wn = W[0] > 0.f ? w / W[0] : w;
-  const float lm = a.p.lm[m];
+  const R wn = W[0] > R(0) ? w / W[0] : w;
+  const R lm = P.lm[m];
   if (PASS == 1) {
     if (a.owner[idx] != m) return;
-    for (int k = 0; k < 3; ++k) a.field[3 * idx + k] = (wn * a.p.lF[3 * m + k]) * lm;
+    for (int k = 0; k < 3; ++k) field[3 * idx + k] = (wn * P.lF[3 * m + k]) * lm;
   } else {
     a.chunks[idx >> 5] = 1;
-    for (int k = 0; k < 3; ++k) atomicAdd(a.field + 3 * idx + k, (wn * a.p.lF[3 * m + k]) * lm);
+    for (int k = 0; k < 3; ++k) atomicAdd(field + 3 * idx + k, (wn * P.lF[3 * m + k]) * lm);
   }
 }
 
@@ -384,9 +431,11 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
 // angle += cw; R from the rotation vector (float64, through the unit
 // quaternion); lx = float32(R X0) + cx.  One block per particle.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles p) {
+template <typename R>
+__global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles pt) {
+  const PView<R> p = pview<R>(pt);
   const int pi = blockIdx.x;
-  const int m0 = p.marker_offset[pi], m1 = p.marker_offset[pi + 1];
+  const int m0 = p.offset[pi], m1 = p.offset[pi + 1];
   // the first marker of this thread is loaded before the rotation is built,
   // so the load latency overlaps it
   int m = m0 + (int)threadIdx.x;
@@ -398,7 +447,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles p
   }
   // every thread builds the same rotation (no shared-memory broadcast)
   double v[3];
-  float ang[3], c[3];
+  R ang[3], c[3];
   for (int k = 0; k < 3; ++k) {
     ang[k] = p.angle[3 * pi + k] + p.cw[3 * pi + k];
     v[k] = ang[k];
@@ -418,13 +467,13 @@ __global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles p
   y /= nq;
   z /= nq;
   w /= nq;
-  const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w),     2 * (x * z + y * w),
+  const double M[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w),     2 * (x * z + y * w),
                        2 * (x * y + z * w),     1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
                        2 * (x * z - y * w),     2 * (y * z + x * w),     1 - 2 * (x * x + y * y)};
   for (; m < m1; m += kRigidThreads) {
     for (int k = 0; k < 3; ++k) {
-      const double r = R[3 * k] * X + R[3 * k + 1] * Y + R[3 * k + 2] * Z;
-      p.lx[3 * m + k] = (float)r + c[k];
+      const double r = M[3 * k] * X + M[3 * k + 1] * Y + M[3 * k + 2] * Z;
+      p.lx[3 * m + k] = (R)r + c[k];
     }
     const int mn = m + kRigidThreads;
     if (mn < m1) {
@@ -445,6 +494,7 @@ struct RunInterp {
     switch (storage) {
       case LBM_STORAGE_FP32: k_interp<Q, LBM_STORAGE_FP32><<<nb, kIbmThreads, 0, s>>>(a); break;
       case LBM_STORAGE_FP16S: k_interp<Q, LBM_STORAGE_FP16S><<<nb, kIbmThreads, 0, s>>>(a); break;
+      case LBM_STORAGE_FP64: k_interp<Q, LBM_STORAGE_FP64><<<nb, kIbmThreads, 0, s>>>(a); break;
       default: k_interp<Q, LBM_STORAGE_BF16S><<<nb, kIbmThreads, 0, s>>>(a); break;
     }
     LBM_LAUNCH_CHECK("ibm_interpolate");
@@ -453,10 +503,43 @@ struct RunInterp {
 };
 
 static int check_particles(const lbm_particles *pt, const char *who) {
-  if (pt == nullptr || pt->n_particles < 0 || pt->n_markers < 0) {
+  if (pt == nullptr || pt->n_particles < 0 || pt->n_markers < 0 ||
+      (pt->fp64 != 0 && pt->fp64 != 1)) {
     set_error("%s: bad particle description", who);
     return LBM_ERR_INVALID;
   }
+  return LBM_OK;
+}
+
+// particle arrays must be float64 exactly when the lattice stores FP64
+static int check_precision(const lbm_lattice *lat, const lbm_particles *pt, const char *who) {
+  const bool any = pt->n_particles > 0 || pt->n_markers > 0;
+  if (any && (lat->storage == LBM_STORAGE_FP64) != (pt->fp64 == 1)) {
+    set_error("%s: particles of an FP64 lattice are float64 (fp64 = 1), otherwise float32", who);
+    return LBM_ERR_INVALID;
+  }
+  return LBM_OK;
+}
+
+// spreading launches (clear, then the claim / write / release passes or the
+// accumulation) in the particles' arithmetic type
+template <typename R>
+static int spread_launch(const SpreadArgs &a, int mode, long long n_markers, cudaStream_t s,
+                         const char *who) {
+  const long long nchunks = (a.g.n + 31) >> 5;
+  k_spread_clear<R><<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, static_cast<R *>(a.field),
+                                                             a.chunks);
+  LBM_LAUNCH_CHECK(who);
+  if (n_markers == 0) return LBM_OK;
+  const unsigned nb = (unsigned)((n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
+  if (mode == 0) {
+    k_spread<0, R><<<nb, kIbmThreads, 0, s>>>(a);
+    k_spread<1, R><<<nb, kIbmThreads, 0, s>>>(a);
+    k_spread<2, R><<<nb, kIbmThreads, 0, s>>>(a);
+  } else {
+    k_spread<3, R><<<nb, kIbmThreads, 0, s>>>(a);
+  }
+  LBM_LAUNCH_CHECK(who);
   return LBM_OK;
 }
 
@@ -544,6 +627,7 @@ int ibm_interpolate(const lbm_lattice *lat, const void *fa, const lbm_force *for
     set_error("ibm_interpolate: WALL_WITH_SPEED faces need face_rho_in");
     return LBM_ERR_INVALID;
   }
+  if ((rc = check_precision(lat, pt, "ibm_interpolate"))) return rc;
   if (pt->n_markers == 0) return LBM_OK;
   InterpArgs a;
   memset(&a, 0, sizeof(a));
@@ -600,7 +684,10 @@ int rigid_wall_and_update(const lbm_lattice *lat, const lbm_particles *pt, int32
   a.dx = dx;
   a.gl = gl;
   a.rouf = rouf;
-  k_rigid<<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
+  if (pt->fp64)
+    k_rigid<double><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
+  else
+    k_rigid<float><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
   LBM_LAUNCH_CHECK("rigid_wall_and_update");
   return LBM_OK;
 }
@@ -618,6 +705,7 @@ int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, fl
     set_error("ibm_spread: field, chunks (and owner in reference mode) are required");
     return LBM_ERR_INVALID;
   }
+  if ((rc = check_precision(lat, pt, "ibm_spread"))) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   SpreadArgs a;
   a.g = make_geom(lat);
@@ -625,27 +713,19 @@ int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, fl
   a.field = field;
   a.chunks = chunks;
   a.owner = owner;
-  const long long nchunks = (a.g.n + 31) >> 5;
-  k_spread_clear<<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, field, chunks);
-  LBM_LAUNCH_CHECK("ibm_spread");
-  if (pt->n_markers == 0) return LBM_OK;
-  const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
-  if (mode == 0) {
-    k_spread<0><<<nb, kIbmThreads, 0, s>>>(a);
-    k_spread<1><<<nb, kIbmThreads, 0, s>>>(a);
-    k_spread<2><<<nb, kIbmThreads, 0, s>>>(a);
-  } else {
-    k_spread<3><<<nb, kIbmThreads, 0, s>>>(a);
-  }
-  LBM_LAUNCH_CHECK("ibm_spread");
-  return LBM_OK;
+  return lat->storage == LBM_STORAGE_FP64
+             ? spread_launch<double>(a, mode, pt->n_markers, s, "ibm_spread")
+             : spread_launch<float>(a, mode, pt->n_markers, s, "ibm_spread");
 }
 
 int rigid_update_markers(const lbm_particles *pt, void *stream) {
   int rc = check_particles(pt, "rigid_update_markers");
   if (rc) return rc;
   if (pt->n_particles == 0) return LBM_OK;
-  k_markers<<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
+  if (pt->fp64)
+    k_markers<double><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
+  else
+    k_markers<float><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
   LBM_LAUNCH_CHECK("rigid_update_markers");
   return LBM_OK;
 }
@@ -672,6 +752,7 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
               n, (int)LBM_SPREAD_NOALLOC_MAX_NODES);
     return LBM_ERR_INVALID;
   }
+  if ((rc = check_precision(lat, pt, "ibm_spread_noalloc"))) return rc;
   int32_t *owner = nullptr;
   int dev = 0;
   bool clean = false;
@@ -683,12 +764,8 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
   a.field = field;
   a.chunks = chunks;
   a.owner = owner;
-  const long long nchunks = (a.g.n + 31) >> 5;
-  k_spread_clear<<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, field, chunks);
-  LBM_LAUNCH_CHECK("ibm_spread_noalloc");
-  if (pt->n_markers == 0) return LBM_OK;
-  const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
-  if (mode == 0) {
+  const bool claims = mode == 0 && pt->n_markers > 0;
+  if (claims) {
     // the claim passes need -1 in every slot they touch; the release pass
     // restores it, so only the first reference-mode call on a device (or
     // one after a failed call) resets the whole array
@@ -699,16 +776,12 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
                       256, 0, s>>>(owner, LBM_SPREAD_NOALLOC_MAX_NODES);
       LBM_LAUNCH_CHECK("ibm_spread_noalloc");
     }
-    k_spread<0><<<nb, kIbmThreads, 0, s>>>(a);
-    k_spread<1><<<nb, kIbmThreads, 0, s>>>(a);
-    k_spread<2><<<nb, kIbmThreads, 0, s>>>(a);
-    LBM_LAUNCH_CHECK("ibm_spread_noalloc");
-    owner_mark(dev, true);
-  } else {
-    k_spread<3><<<nb, kIbmThreads, 0, s>>>(a);
-    LBM_LAUNCH_CHECK("ibm_spread_noalloc");
   }
-  return LBM_OK;
+  rc = lat->storage == LBM_STORAGE_FP64
+           ? spread_launch<double>(a, mode, pt->n_markers, s, "ibm_spread_noalloc")
+           : spread_launch<float>(a, mode, pt->n_markers, s, "ibm_spread_noalloc");
+  if (rc == LBM_OK && claims) owner_mark(dev, true);
+  return rc;
 }
 
 }  // extern "C"

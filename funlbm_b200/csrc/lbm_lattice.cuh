@@ -57,6 +57,8 @@ struct VSet;
     return speed2(i) == 0 ? (W0) : speed2(i) == 1 ? (W1) : speed2(i) == 2 ? (W2) : (W3); \
   }                                                                                       \
   __host__ __device__ static constexpr float w(int i) { return (float)wd(i); }           \
+  template <typename R>                                                                   \
+  __host__ __device__ static constexpr R wr(int i) { return (R)wd(i); }                   \
   __host__ __device__ static constexpr int rev(int i) {                                   \
     int r = 0;                                                                            \
     for (int j = 0; j < QN; ++j)                                                          \
@@ -121,6 +123,7 @@ struct Storage;
 template <>
 struct Storage<LBM_STORAGE_FP32> {
   using T = float;
+  using R = float;   // arithmetic type of the kernels
   static constexpr int kBits = 32;
   static constexpr bool kDev = false;
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
@@ -133,6 +136,7 @@ struct Storage<LBM_STORAGE_FP32> {
 template <>
 struct Storage<LBM_STORAGE_FP16S> {
   using T = __half;
+  using R = float;
   static constexpr int kBits = 16;
   static constexpr bool kDev = true;
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
@@ -149,6 +153,7 @@ struct Storage<LBM_STORAGE_FP16S> {
 template <>
 struct Storage<LBM_STORAGE_BF16S> {
   using T = __nv_bfloat16;
+  using R = float;
   static constexpr int kBits = 16;
   static constexpr bool kDev = true;
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
@@ -161,6 +166,22 @@ struct Storage<LBM_STORAGE_BF16S> {
   __device__ __forceinline__ static void store(T *p, float v, float w) {
     *p = __float2bfloat16_rn(v - w);
   }
+};
+
+// FP64: populations, moments, forcing and collision in double -- the
+// comparison run against which the float32 and 16-bit storages are measured.
+template <>
+struct Storage<LBM_STORAGE_FP64> {
+  using T = double;
+  using R = double;
+  static constexpr int kBits = 64;
+  static constexpr bool kDev = false;
+  __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
+  __device__ __forceinline__ static double cvt(T v) { return v; }
+  __device__ __forceinline__ static double work(const T *p) { return __ldg(p); }
+  __device__ __forceinline__ static void put(T *p, double v) { *p = v; }
+  __device__ __forceinline__ static double load(const T *p, double) { return __ldg(p); }
+  __device__ __forceinline__ static void store(T *p, double v, double) { *p = v; }
 };
 
 // Raw 16 bits of one stored element.
@@ -241,6 +262,30 @@ struct Geom {
   float tau, inv_tau, cs2, inv_cs2, inv_cs4, force_c;  // force_c = 1 - 1/(2 tau)
   float re_mu;
   const double *neq_profile;
+  // the same constants in double, for FP64 storage: tau as given, cs^2 =
+  // double(sqrt(1/3))^2, wall velocities widened
+  double inv_tau_d, inv_cs2_d, inv_cs4_d, force_c_d;
+  double uw_d[LBM_NFACES][3];
+};
+
+// Lattice constants in the arithmetic type R of a kernel.
+template <typename R>
+struct Cst;
+template <>
+struct Cst<float> {
+  __device__ __forceinline__ static float inv_tau(const Geom &g) { return g.inv_tau; }
+  __device__ __forceinline__ static float inv_cs2(const Geom &g) { return g.inv_cs2; }
+  __device__ __forceinline__ static float inv_cs4(const Geom &g) { return g.inv_cs4; }
+  __device__ __forceinline__ static float force_c(const Geom &g) { return g.force_c; }
+  __device__ __forceinline__ static float uw(const Geom &g, int fc, int k) { return g.uw[fc][k]; }
+};
+template <>
+struct Cst<double> {
+  __device__ __forceinline__ static double inv_tau(const Geom &g) { return g.inv_tau_d; }
+  __device__ __forceinline__ static double inv_cs2(const Geom &g) { return g.inv_cs2_d; }
+  __device__ __forceinline__ static double inv_cs4(const Geom &g) { return g.inv_cs4_d; }
+  __device__ __forceinline__ static double force_c(const Geom &g) { return g.force_c_d; }
+  __device__ __forceinline__ static double uw(const Geom &g, int fc, int k) { return g.uw_d[fc][k]; }
 };
 
 // face-plane index of node (x, y, z) on face `fc`
@@ -277,10 +322,11 @@ __device__ __forceinline__ bool on_any_face(const Geom &g, int x, int y, int z) 
 // WORK: return the storage's working value (d for the shifted forms) instead
 // of f; the WALL_WITH_SPEED correction is the same in both.
 template <int Q, int S, int I, bool WORK = false>
-__device__ __forceinline__ float pull_one(const typename Storage<S>::T *__restrict__ fa,
-                                          const Geom &g, int x, int y, int z,
-                                          const float *__restrict__ face_rho) {
+__device__ __forceinline__ typename Storage<S>::R pull_one(
+    const typename Storage<S>::T *__restrict__ fa, const Geom &g, int x, int y, int z,
+    const typename Storage<S>::R *__restrict__ face_rho) {
   using V = VSet<Q>;
+  using R = typename Storage<S>::R;
   constexpr int ex = V::ex(I), ey = V::ey(I), ez = V::ez(I);
   int fc = -1;
   if (ex > 0 && x == 0) fc = 0;
@@ -290,7 +336,7 @@ __device__ __forceinline__ float pull_one(const typename Storage<S>::T *__restri
   if (ez > 0 && z == 0) fc = 4;
   if (ez < 0 && z == g.nz - 1) fc = 5;
   int sx = x - ex, sy = y - ey, sz = z - ez, sd = I;
-  float corr = 0.f;
+  R corr = R(0);
   if (fc >= 0) {
     const int code = g.face[fc];
     sx = x;
@@ -305,14 +351,15 @@ __device__ __forceinline__ float pull_one(const typename Storage<S>::T *__restri
     } else {
       sd = V::rev(I);
       if (code == LBM_BC_WALL_WITH_SPEED) {
-        const float rho_t = face_rho[plane_index(g, fc, x, y, z)];
-        const float eu = (float)ex * g.uw[fc][0] + (float)ey * g.uw[fc][1] + (float)ez * g.uw[fc][2];
-        corr = 2.f * (rho_t * V::w(I)) * eu * g.inv_cs2;
+        const R rho_t = face_rho[plane_index(g, fc, x, y, z)];
+        const R eu = (R)ex * Cst<R>::uw(g, fc, 0) + (R)ey * Cst<R>::uw(g, fc, 1) +
+                     (R)ez * Cst<R>::uw(g, fc, 2);
+        corr = R(2) * (rho_t * V::template wr<R>(I)) * eu * Cst<R>::inv_cs2(g);
       }
     }
   }
   const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;
-  const float w_sd = sd == I ? V::w(I) : V::w(V::rev(I));
+  const R w_sd = sd == I ? V::template wr<R>(I) : V::template wr<R>(V::rev(I));
   if constexpr (WORK)
     return Storage<S>::work(fa + (long long)sd * g.n + src) - corr;
   else
@@ -321,24 +368,27 @@ __device__ __forceinline__ float pull_one(const typename Storage<S>::T *__restri
 
 template <int Q, int S, bool WORK, int I = 0>
 struct PullGeneral {
+  using R = typename Storage<S>::R;
   __device__ __forceinline__ static void run(const typename Storage<S>::T *__restrict__ fa,
                                              const Geom &g, int x, int y, int z,
-                                             const float *__restrict__ face_rho, float f[Q]) {
+                                             const R *__restrict__ face_rho, R f[Q]) {
     f[I] = pull_one<Q, S, I, WORK>(fa, g, x, y, z, face_rho);
     PullGeneral<Q, S, WORK, I + 1>::run(fa, g, x, y, z, face_rho, f);
   }
 };
 template <int Q, int S, bool WORK>
 struct PullGeneral<Q, S, WORK, Q> {
+  using R = typename Storage<S>::R;
   __device__ __forceinline__ static void run(const typename Storage<S>::T *__restrict__,
                                              const Geom &, int, int, int,
-                                             const float *__restrict__, float *) {}
+                                             const R *__restrict__, R *) {}
 };
 
 template <int Q, int S, bool WORK = false>
 __device__ __forceinline__ void pull_general(const typename Storage<S>::T *__restrict__ fa,
                                              const Geom &g, int x, int y, int z,
-                                             const float *__restrict__ face_rho, float f[Q]) {
+                                             const typename Storage<S>::R *__restrict__ face_rho,
+                                             typename Storage<S>::R f[Q]) {
   PullGeneral<Q, S, WORK>::run(fa, g, x, y, z, face_rho, f);
 }
 
@@ -364,18 +414,18 @@ struct StepPlanes {
 // WALL_WITH_SPEED correction of the directions entering through z face FC
 // (4 = bottom, 5 = top) at a node of an interior row, applied after the
 // plain bounce-back pull: the same expression as pull_one's.
-template <int Q, int FC>
-__device__ __forceinline__ void zface_wws(const Geom &g, const float *__restrict__ face_rho,
-                                          int x, int y, int z, float f[Q]) {
+template <int Q, int FC, typename R>
+__device__ __forceinline__ void zface_wws(const Geom &g, const R *__restrict__ face_rho,
+                                          int x, int y, int z, R f[Q]) {
   using V = VSet<Q>;
-  const float rho_t = face_rho[plane_index(g, FC, x, y, z)];
+  const R rho_t = face_rho[plane_index(g, FC, x, y, z)];
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     constexpr int ez = V::ez(i);
     if constexpr ((FC == 4 && ez > 0) || (FC == 5 && ez < 0)) {
-      const float eu = (float)V::ex(i) * g.uw[FC][0] + (float)V::ey(i) * g.uw[FC][1] +
-                       (float)ez * g.uw[FC][2];
-      f[i] = f[i] - 2.f * (rho_t * V::w(i)) * eu * g.inv_cs2;
+      const R eu = (R)V::ex(i) * Cst<R>::uw(g, FC, 0) + (R)V::ey(i) * Cst<R>::uw(g, FC, 1) +
+                   (R)ez * Cst<R>::uw(g, FC, 2);
+      f[i] = f[i] - R(2) * (rho_t * V::template wr<R>(i)) * eu * Cst<R>::inv_cs2(g);
     }
   });
 }
@@ -388,8 +438,9 @@ __device__ __forceinline__ void zface_wws(const Geom &g, const float *__restrict
 // pull_general.
 template <int Q, int S, bool WORK>
 __device__ __forceinline__ void pull_row_node(const StepPlanes &p, const Geom &g,
-                                              const float *__restrict__ face_rho, unsigned idx,
-                                              int x, int y, int z, float f[Q]) {
+                                              const typename Storage<S>::R *__restrict__ face_rho,
+                                              unsigned idx, int x, int y, int z,
+                                              typename Storage<S>::R f[Q]) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
@@ -404,7 +455,7 @@ __device__ __forceinline__ void pull_row_node(const StepPlanes &p, const Geom &g
     if constexpr (WORK)
       f[i] = St::work(src);
     else
-      f[i] = St::load(src, V::w(i));
+      f[i] = St::load(src, V::template wr<typename St::R>(i));
   });
   if (bottom && g.face[4] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 4>(g, face_rho, x, y, z, f);
   if (top && g.face[5] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 5>(g, face_rho, x, y, z, f);
@@ -432,21 +483,23 @@ __device__ __forceinline__ float pull_rolled(const typename Storage<S>::T *__res
 // below is explicit (__fmaf_rn), so each kernel that calls these functions
 // produces the same bits whatever its launch shape.
 // ---------------------------------------------------------------------------
-#define LBM_FMA(a, b, c) __fmaf_rn((a), (b), (c))
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+#define LBM_FMA(a, b, c) ::lbm::fma_rn((a), (b), (c))
 
 // Moments (flow/d3/base.py:116-133): rho = sum f, u = (sum f e + F/2) / rho,
 // u := 0 on all six boundary planes whatever their condition.
-template <int Q>
-__device__ __forceinline__ void moments(const float f[Q], float fx, float fy, float fz,
-                                        bool face, float &rho, float &ux, float &uy, float &uz) {
+template <int Q, typename R>
+__device__ __forceinline__ void moments(const R f[Q], R fx, R fy, R fz, bool face, R &rho, R &ux,
+                                        R &uy, R &uz) {
   using V = VSet<Q>;
-  float r = f[0], jx = 0.f, jy = 0.f, jz = 0.f;
+  R r = f[0], jx = R(0), jy = R(0), jz = R(0);
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     constexpr int j = V::rev(i);
     if constexpr (i != 0 && i < j) {
-      const float s = f[i] + f[j];
-      const float d = f[i] - f[j];
+      const R s = f[i] + f[j];
+      const R d = f[i] - f[j];
       r += s;
       if constexpr (V::ex(i) > 0) jx += d;
       if constexpr (V::ex(i) < 0) jx -= d;
@@ -457,19 +510,19 @@ __device__ __forceinline__ void moments(const float f[Q], float fx, float fy, fl
     }
   });
   rho = r;
-  const float inv = 1.f / r;
-  ux = face ? 0.f : LBM_FMA(0.5f, fx, jx) * inv;
-  uy = face ? 0.f : LBM_FMA(0.5f, fy, jy) * inv;
-  uz = face ? 0.f : LBM_FMA(0.5f, fz, jz) * inv;
+  const R inv = R(1) / r;
+  ux = face ? R(0) : LBM_FMA(R(0.5), fx, jx) * inv;
+  uy = face ? R(0) : LBM_FMA(R(0.5), fy, jy) * inv;
+  uz = face ? R(0) : LBM_FMA(R(0.5), fz, jz) * inv;
 }
 
 // e_i . v with e_i in {-1, 0, 1}^3, folded at compile time
-template <int Q, int I>
-__device__ __forceinline__ float edot(float vx, float vy, float vz) {
+template <int Q, int I, typename R>
+__device__ __forceinline__ R edot(R vx, R vy, R vz) {
   using V = VSet<Q>;
-  float r = 0.f;
+  R r = R(0);
   bool first = true;
-  auto acc = [&](int e, float v) {
+  auto acc = [&](int e, R v) {
     if (e == 0) return;
     if (first) {
       r = e > 0 ? v : -v;
@@ -488,27 +541,28 @@ __device__ __forceinline__ float edot(float vx, float vy, float vz) {
 //   f_i += (1 - 1/(2 tau)) w_i [ (e_i - u)/cs^2 + (u o e_i) o e_i / cs^4 ] . F
 // (component-wise u_k e_ik^2, the reference's form).  For the pair (i, j),
 // e_j = -e_i: the e.F part flips sign, the rest is shared.
-template <int Q>
-__device__ __forceinline__ void add_force(float f[Q], const Geom &g, float ux, float uy, float uz,
-                                          float fx, float fy, float fz) {
+template <int Q, typename R>
+__device__ __forceinline__ void add_force(R f[Q], const Geom &g, R ux, R uy, R uz, R fx, R fy,
+                                          R fz) {
   using V = VSet<Q>;
-  const float uF = LBM_FMA(ux, fx, LBM_FMA(uy, fy, uz * fz));
-  const float ax = ux * fx, ay = uy * fy, az = uz * fz;
-  const float base = -uF * g.inv_cs2;
+  const R inv_cs2 = Cst<R>::inv_cs2(g), force_c = Cst<R>::force_c(g);
+  const R uF = LBM_FMA(ux, fx, LBM_FMA(uy, fy, uz * fz));
+  const R ax = ux * fx, ay = uy * fy, az = uz * fz;
+  const R base = -uF * inv_cs2;
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     constexpr int j = V::rev(i);
-    constexpr float cw = V::w(i);
+    constexpr R cw = V::template wr<R>(i);
     if constexpr (i == 0) {
-      f[0] = LBM_FMA(g.force_c * cw, base, f[0]);
+      f[0] = LBM_FMA(force_c * cw, base, f[0]);
     } else if constexpr (i < j) {
-      float t2 = 0.f;
+      R t2 = R(0);
       if constexpr (V::ex(i) != 0) t2 += ax;
       if constexpr (V::ey(i) != 0) t2 += ay;
       if constexpr (V::ez(i) != 0) t2 += az;
-      const float shared = LBM_FMA(t2, g.inv_cs4, base);
-      const float eF = edot<Q, i>(fx, fy, fz) * g.inv_cs2;
-      const float c = g.force_c * cw;
+      const R shared = LBM_FMA(t2, Cst<R>::inv_cs4(g), base);
+      const R eF = edot<Q, i>(fx, fy, fz) * inv_cs2;
+      const R c = force_c * cw;
       f[i] = LBM_FMA(c, shared + eF, f[i]);
       f[j] = LBM_FMA(c, shared - eF, f[j]);
     }
@@ -528,25 +582,25 @@ __device__ __forceinline__ float feq_of(const Geom &g, int i, float rho, float u
   return LBM_FMA(0.5f * t, t, (1.f - u2) + t) * (rho * V::w(i));
 }
 
-template <int Q>
-__device__ __forceinline__ void collide(float f[Q], const Geom &g, float rho, float ux, float uy,
-                                        float uz) {
+template <int Q, typename R>
+__device__ __forceinline__ void collide(R f[Q], const Geom &g, R rho, R ux, R uy, R uz) {
   using V = VSet<Q>;
-  const float u2 = LBM_FMA(ux, ux, LBM_FMA(uy, uy, uz * uz)) * (0.5f * g.inv_cs2);
-  const float om = g.inv_tau, keep = 1.f - g.inv_tau;
-  const float orho = om * rho;
-  const float one_u2 = 1.f - u2;
+  const R inv_cs2 = Cst<R>::inv_cs2(g), inv_tau = Cst<R>::inv_tau(g);
+  const R u2 = LBM_FMA(ux, ux, LBM_FMA(uy, uy, uz * uz)) * (R(0.5) * inv_cs2);
+  const R om = inv_tau, keep = R(1) - inv_tau;
+  const R orho = om * rho;
+  const R one_u2 = R(1) - u2;
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     constexpr int j = V::rev(i);
-    constexpr float w = V::w(i);
+    constexpr R w = V::template wr<R>(i);
     if constexpr (i == 0) {
       f[0] = LBM_FMA(f[0], keep, (orho * w) * one_u2);
     } else if constexpr (i < j) {
-      const float t = edot<Q, i>(ux, uy, uz) * g.inv_cs2;
-      const float ow = orho * w;
-      const float a = ow * LBM_FMA(0.5f * t, t, one_u2);
-      const float b = ow * t;
+      const R t = edot<Q, i>(ux, uy, uz) * inv_cs2;
+      const R ow = orho * w;
+      const R a = ow * LBM_FMA(R(0.5) * t, t, one_u2);
+      const R b = ow * t;
       f[i] = LBM_FMA(f[i], keep, a + b);
       f[j] = LBM_FMA(f[j], keep, a - b);
     }
@@ -616,10 +670,11 @@ __device__ __forceinline__ void collide_dev(float d[Q], const Geom &g, float rho
   });
 }
 
-__device__ __forceinline__ void flag_bad(unsigned *status, float rho, float ux, float uy, float uz) {
+template <typename R>
+__device__ __forceinline__ void flag_bad(unsigned *status, R rho, R ux, R uy, R uz) {
   if (status == nullptr) return;
-  if (!(rho > 0.f) || !(rho < 3.0e38f)) atomicOr(status, LBM_STATUS_RHO_BAD);
-  if (!(fabsf(ux) + fabsf(uy) + fabsf(uz) < 3.0e38f)) atomicOr(status, LBM_STATUS_U_BAD);
+  if (!(rho > R(0)) || !(rho < R(3.0e38))) atomicOr(status, LBM_STATUS_RHO_BAD);
+  if (!(fabs(ux) + fabs(uy) + fabs(uz) < R(3.0e38))) atomicOr(status, LBM_STATUS_U_BAD);
 }
 
 }  // namespace lbm

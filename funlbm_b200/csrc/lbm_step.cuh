@@ -21,18 +21,19 @@ struct StepArgs {
   const void *fa;
   void *fb;
   float go[3], gn[3];
-  const float *fol_old, *fol_new;
+  // fields, face densities and observation buffers hold the storage's
+  // arithmetic type (float64 for LBM_STORAGE_FP64, float32 otherwise)
+  const void *fol_old, *fol_new;
   const uint8_t *ch_old, *ch_new;
-  const float *face_rho_in;
-  float *face_rho_out;
-  float *obs_f, *obs_rho, *obs_u;
+  const void *face_rho_in;
+  void *face_rho_out;
+  void *obs_f, *obs_rho, *obs_u;
   unsigned *status;
   StepPlanes p;
 };
 
-template <int Q>
-__device__ __forceinline__ void write_face_rho(const Geom &g, float *out, int x, int y, int z,
-                                               float rho) {
+template <int Q, typename R>
+__device__ __forceinline__ void write_face_rho(const Geom &g, R *out, int x, int y, int z, R rho) {
   if (x == 0) out[plane_index(g, 0, x, y, z)] = rho;
   if (x == g.nx - 1) out[plane_index(g, 1, x, y, z)] = rho;
   if (y == 0) out[plane_index(g, 2, x, y, z)] = rho;
@@ -41,10 +42,11 @@ __device__ __forceinline__ void write_face_rho(const Geom &g, float *out, int x,
   if (z == g.nz - 1) out[plane_index(g, 5, x, y, z)] = rho;
 }
 
-__device__ __forceinline__ unsigned bad_bits(float rho, float ux, float uy, float uz) {
+template <typename R>
+__device__ __forceinline__ unsigned bad_bits(R rho, R ux, R uy, R uz) {
   unsigned b = 0;
-  if (!(rho > 0.f) || !(rho < 3.0e38f)) b |= LBM_STATUS_RHO_BAD;
-  if (!(fabsf(ux) + fabsf(uy) + fabsf(uz) < 3.0e38f)) b |= LBM_STATUS_U_BAD;
+  if (!(rho > R(0)) || !(rho < R(3.0e38))) b |= LBM_STATUS_RHO_BAD;
+  if (!(fabs(ux) + fabs(uy) + fabs(uz) < R(3.0e38))) b |= LBM_STATUS_U_BAD;
   return b;
 }
 
@@ -70,24 +72,26 @@ __device__ __forceinline__ ChunkForce chunk_force(const StepArgs &a, unsigned id
   return c;
 }
 
-template <int Q, bool FORCE, bool DEV>
-__device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsigned idx, int x,
+template <int Q, bool FORCE, bool DEV, typename R>
+__device__ __forceinline__ void finish_node(const StepArgs &a, R f[Q], unsigned idx, int x,
                                             int y, int z, bool face, ChunkForce cf,
                                             unsigned &bad) {
   using V = VSet<Q>;
-  float fox = a.go[0], foy = a.go[1], foz = a.go[2];
-  float fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
+  R fox = a.go[0], foy = a.go[1], foz = a.go[2];
+  R fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
   if (cf.old_here) {
-    fox += a.fol_old[3ull * idx];
-    foy += a.fol_old[3ull * idx + 1];
-    foz += a.fol_old[3ull * idx + 2];
+    const R *fol = static_cast<const R *>(a.fol_old);
+    fox += fol[3ull * idx];
+    foy += fol[3ull * idx + 1];
+    foz += fol[3ull * idx + 2];
   }
   if (cf.new_here) {
-    fnx += a.fol_new[3ull * idx];
-    fny += a.fol_new[3ull * idx + 1];
-    fnz += a.fol_new[3ull * idx + 2];
+    const R *fol = static_cast<const R *>(a.fol_new);
+    fnx += fol[3ull * idx];
+    fny += fol[3ull * idx + 1];
+    fnz += fol[3ull * idx + 2];
   }
-  float rho, drho = 0.f, ux, uy, uz;
+  R rho, drho = R(0), ux, uy, uz;
   if constexpr (DEV)
     dev_moments<Q>(f, fox, foy, foz, face, rho, drho, ux, uy, uz);
   else
@@ -97,8 +101,8 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsig
   // nothing and the second moment pass repeats the first, so such nodes skip
   // them -- the same rule in every kernel.  (A zero new force alone is not
   // enough: the second pass drops the previous force from u.)
-  if (FORCE && (fnx != 0.f || fny != 0.f || fnz != 0.f || fox != 0.f || foy != 0.f ||
-                foz != 0.f)) {
+  if (FORCE && (fnx != R(0) || fny != R(0) || fnz != R(0) || fox != R(0) || foy != R(0) ||
+                foz != R(0))) {
     add_force<Q>(f, a.g, ux, uy, uz, fnx, fny, fnz);
     if constexpr (DEV)
       dev_moments<Q>(f, fnx, fny, fnz, face, rho, drho, ux, uy, uz);
@@ -106,18 +110,21 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, float f[Q], unsig
       moments<Q>(f, fnx, fny, fnz, face, rho, ux, uy, uz);
   }
   bad |= bad_bits(rho, ux, uy, uz);
-  if (face && a.face_rho_out != nullptr) write_face_rho<Q>(a.g, a.face_rho_out, x, y, z, rho);
+  if (face && a.face_rho_out != nullptr)
+    write_face_rho<Q>(a.g, static_cast<R *>(a.face_rho_out), x, y, z, rho);
   if (a.obs_f != nullptr) {
+    R *of = static_cast<R *>(a.obs_f);
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      a.obs_f[(long long)i * a.g.n + idx] = DEV ? f[i] + V::w(i) : f[i];
+      of[(long long)i * a.g.n + idx] = DEV ? f[i] + V::template wr<R>(i) : f[i];
     });
   }
-  if (a.obs_rho != nullptr) a.obs_rho[idx] = rho;
+  if (a.obs_rho != nullptr) static_cast<R *>(a.obs_rho)[idx] = rho;
   if (a.obs_u != nullptr) {
-    a.obs_u[3ull * idx] = ux;
-    a.obs_u[3ull * idx + 1] = uy;
-    a.obs_u[3ull * idx + 2] = uz;
+    R *ou = static_cast<R *>(a.obs_u);
+    ou[3ull * idx] = ux;
+    ou[3ull * idx + 1] = uy;
+    ou[3ull * idx + 2] = uz;
   }
   if (a.fb != nullptr) {
     if constexpr (DEV)
@@ -145,12 +152,14 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   int x, y, z;
   const ChunkForce cf = chunk_force<FORCE>(a, idx);
   a.dec(idx, x, y, z);
+  using R = typename St::R;
+  const R *face_rho = static_cast<const R *>(a.face_rho_in);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
-  float f[Q];
+  R f[Q];
   if (row_in)
-    pull_row_node<Q, S, true>(a.p, a.g, a.face_rho_in, idx, x, y, z, f);
+    pull_row_node<Q, S, true>(a.p, a.g, face_rho, idx, x, y, z, f);
   else
-    pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, a.face_rho_in, f);
+    pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, face_rho, f);
   unsigned bad = 0;
   finish_node<Q, FORCE, St::kDev>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1, cf,
                                   bad);
@@ -204,12 +213,14 @@ __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0,
                                                int y, int z0) {
   using St = Storage<S>;
   using T = typename St::T;
+  using R = typename St::R;
   const T *fa = static_cast<const T *>(a.fa);
+  const R *face_rho = static_cast<const R *>(a.face_rho_in);
   unsigned bad = 0;
 #pragma unroll 1
   for (int k = 0; k < count; ++k) {
-    float f[Q];
-    pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, a.face_rho_in, f);
+    R f[Q];
+    pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, face_rho, f);
     // the nodes may lie in two chunks (pairs of odd-length rows)
     finish_node<Q, FORCE, St::kDev>(a, f, idx0 + k, x, y, z0 + k, true,
                                     chunk_force<FORCE>(a, idx0 + k), bad);
@@ -296,13 +307,14 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
         }
       });
       if (pr == 0 && bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
-        zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f0);
+        zface_wws<Q, 4>(a.g, static_cast<const float *>(a.face_rho_in), x, y, 0, f0);
       if (pr == kWords - 1 && top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
-        zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, a.g.nz - 1, f1);
+        zface_wws<Q, 5>(a.g, static_cast<const float *>(a.face_rho_in), x, y, a.g.nz - 1, f1);
     } else if constexpr (!kCompact) {
       const T *fa = static_cast<const T *>(a.fa);
-      pull_general<Q, S, true>(fa, a.g, x, y, za, a.face_rho_in, f0);
-      pull_general<Q, S, true>(fa, a.g, x, y, za + 1, a.face_rho_in, f1);
+      const float *face_rho = static_cast<const float *>(a.face_rho_in);
+      pull_general<Q, S, true>(fa, a.g, x, y, za, face_rho, f0);
+      pull_general<Q, S, true>(fa, a.g, x, y, za + 1, face_rho, f1);
     }
     finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
                                 !row_in || za == 0 || za == a.g.nz - 1, cf, bad);
@@ -340,6 +352,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
     step_vec_pairs<Q, S, FORCE, NZ, COMPACT>(a, t);
     return;
   }
+  using R = typename St::R;
   constexpr int kWords = NZ * St::kBits / 32;
   const unsigned idx0 = t * NZ;
   if (idx0 >= (unsigned)a.g.n) return;
@@ -355,7 +368,8 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
     }
     row_in = true;
   }
-  float f[NZ][Q];
+  const R *face_rho = static_cast<const R *>(a.face_rho_in);
+  R f[NZ][Q];
   if (row_in) {
     const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
     static_for<Q>([&](auto ic) {
@@ -363,10 +377,13 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
       constexpr int ez = V::ez(i);
       const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
       const Words<kWords> raw = ld_words<kWords>(ps);
-      float v[NZ];
+      R v[NZ];
       if constexpr (St::kBits == 32) {
 #pragma unroll
         for (int k = 0; k < NZ; ++k) v[k] = __uint_as_float(raw.w[k]);
+      } else if constexpr (St::kBits == 64) {
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) v[k] = __hiloint2double((int)raw.w[2 * k + 1], (int)raw.w[2 * k]);
       } else {
 #pragma unroll
         for (int k = 0; k < NZ / 2; ++k) {
@@ -390,14 +407,14 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
       }
     });
     if (bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
-      zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f[0]);
+      zface_wws<Q, 4>(a.g, face_rho, x, y, 0, f[0]);
     if (top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
-      zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, a.g.nz - 1, f[NZ - 1]);
+      zface_wws<Q, 5>(a.g, face_rho, x, y, a.g.nz - 1, f[NZ - 1]);
   } else if constexpr (!kCompact) {
     const T *fa = static_cast<const T *>(a.fa);
 #pragma unroll
     for (int k = 0; k < NZ; ++k)
-      pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, a.face_rho_in, f[k]);
+      pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, face_rho, f[k]);
   }
 
   unsigned bad = 0;
@@ -415,6 +432,12 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
     if constexpr (St::kBits == 32) {
 #pragma unroll
       for (int k = 0; k < NZ; ++k) raw.w[k] = __float_as_uint(f[k][i]);
+    } else if constexpr (St::kBits == 64) {
+#pragma unroll
+      for (int k = 0; k < NZ; ++k) {
+        raw.w[2 * k] = (unsigned)__double2loint(f[k][i]);
+        raw.w[2 * k + 1] = (unsigned)__double2hiint(f[k][i]);
+      }
     } else {
 #pragma unroll
       for (int k = 0; k < NZ / 2; ++k) raw.w[k] = put2<S>(f[2 * k][i], f[2 * k + 1][i]);
@@ -432,7 +455,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
 // FP32 runs uncapped.
 template <int Q, int S, int NZ, bool FORCE>
 constexpr int vec_reg_cap() {
-  if (Storage<S>::kBits == 32) return 0;
+  if (Storage<S>::kBits != 16) return 0;
   if (NZ == 2 && FORCE) return Q == 19 ? 72 : Q == 27 ? 96 : 0;
   if (NZ == 4) return Q == 15 || Q == 19 ? 128 : 0;
   return 0;
@@ -573,6 +596,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
   const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
   const int R = p.rows_per_stage;
   const T *__restrict__ fa = static_cast<const T *>(a.fa);
+  const float *face_rho = static_cast<const float *>(a.face_rho_in);
   const int tid = threadIdx.x;
   const long long G = gridDim.x;
   if (tid == 0) {
@@ -663,12 +687,12 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
           }
         });
         if (z == 0 && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
-          zface_wws<Q, 4>(a.g, a.face_rho_in, x, y, 0, f0);
+          zface_wws<Q, 4>(a.g, face_rho, x, y, 0, f0);
         if (z + 2 == nz && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
-          zface_wws<Q, 5>(a.g, a.face_rho_in, x, y, nz - 1, f1);
+          zface_wws<Q, 5>(a.g, face_rho, x, y, nz - 1, f1);
       } else {
-        pull_general<Q, S, true>(fa, a.g, x, y, z, a.face_rho_in, f0);
-        pull_general<Q, S, true>(fa, a.g, x, y, z + 1, a.face_rho_in, f1);
+        pull_general<Q, S, true>(fa, a.g, x, y, z, face_rho, f0);
+        pull_general<Q, S, true>(fa, a.g, x, y, z + 1, face_rho, f1);
       }
       unsigned bad = 0;
       finish_node<Q, FORCE, St::kDev>(a, f0, idx, x, y, z, !row_in || z == 0, cf, bad);
@@ -794,7 +818,12 @@ struct StepLauncher {
     return LBM_OK;
   }
   static int go_tma(const StepArgs &a, bool force, cudaStream_t s) {
-    return force ? go_tma_f<true>(a, s) : go_tma_f<false>(a, s);
+    if constexpr (Storage<S>::kBits == 64) {
+      set_error("lbm_flow_step: row staging is not built for FP64 storage");
+      return LBM_ERR_UNSUPPORTED;
+    } else {
+      return force ? go_tma_f<true>(a, s) : go_tma_f<false>(a, s);
+    }
   }
 
   template <int NZ, int TB>
@@ -851,9 +880,11 @@ struct StepLauncher {
       go_nz<2>(a, force, threads, s);
       return LBM_OK;
     }
-    if (nodes == 4) {
-      go_nz<4>(a, force, threads, s);
-      return LBM_OK;
+    if constexpr (bits != 64) {
+      if (nodes == 4) {
+        go_nz<4>(a, force, threads, s);
+        return LBM_OK;
+      }
     }
     if constexpr (bits == 16) {
       if (nodes == 8) {
@@ -880,11 +911,13 @@ int run_step_batch_qs(const StepArgs *entries, const unsigned *block_begin, int 
       k_step_batch<Q, S, true, 2, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
     else
       k_step_batch<Q, S, false, 2, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
-  } else if (nodes == 4) {
-    if (force)
-      k_step_batch<Q, S, true, 4, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
-    else
-      k_step_batch<Q, S, false, 4, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
+  } else if (nodes == 4 && Storage<S>::kBits != 64) {
+    if constexpr (Storage<S>::kBits != 64) {
+      if (force)
+        k_step_batch<Q, S, true, 4, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
+      else
+        k_step_batch<Q, S, false, 4, 128><<<total_blocks, 128, 0, s>>>(entries, block_begin, count);
+    }
   } else {
     if (force)
       k_step_batch<Q, S, true, 1, 256><<<total_blocks, 256, 0, s>>>(entries, block_begin, count);
@@ -906,8 +939,8 @@ int run_step_qs(const StepArgs &a, bool force, int nodes, int threads, cudaStrea
   return LBM_OK;
 }
 
-#define LBM_FOR_EACH_QS(X) \
-  X(13, 0) X(13, 1) X(13, 2) X(15, 0) X(15, 1) X(15, 2) X(19, 0) X(19, 1) X(19, 2) X(27, 0) \
-  X(27, 1) X(27, 2)
+#define LBM_FOR_EACH_QS(X)                                                                  \
+  X(13, 0) X(13, 1) X(13, 2) X(13, 3) X(15, 0) X(15, 1) X(15, 2) X(15, 3) X(19, 0) X(19, 1) \
+  X(19, 2) X(19, 3) X(27, 0) X(27, 1) X(27, 2) X(27, 3)
 
 }  // namespace lbm

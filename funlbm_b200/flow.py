@@ -211,6 +211,10 @@ class FlowD3(Flow):
         self._lat = Lattice(q, (X, Y, Z), codes, tau_float32(self.config.mu), storage=storage,
                             face_uw=uw, re_mu=re_mu, device=self.device, allocate=False)
         dev = self.device
+        self._fp64 = storage == "fp64"
+        if self._fp64:
+            self._init_fp64()
+            return
         self._f = self.param.w.reshape(q, 1).expand(q, self.n).contiguous()
         self._f2 = None
         self._feq = None
@@ -226,14 +230,60 @@ class FlowD3(Flow):
             self._f = self.initial_field(self.config.init_field)
             self.update_u_rou()
 
-    def initial_field(self, spec):
-        """f = feq(rho = 1, u0) of the ``init_field`` extension (float32 SoA)."""
+    def initial_field(self, spec, dtype=torch.float32):
+        """f = feq(rho = 1, u0) of the ``init_field`` extension (SoA, float32
+        or float64)."""
         kind = (spec.get("type") if isinstance(spec, dict) else spec) or "taylor_green"
         if kind != "taylor_green":
             raise ValueError("unknown init_field type %r" % (kind,))
         u0 = float(spec.get("u0", 0.05)) if isinstance(spec, dict) else 0.05
-        u = taylor_green_velocity(self.shape, u0, self.device)
-        return equilibrium_soa(self.param, u, torch.ones(self.shape + (1,), device=self.device))
+        u = taylor_green_velocity(self.shape, u0, self.device, dtype=dtype)
+        if dtype == torch.float32:
+            return equilibrium_soa(self.param, u, torch.ones(self.shape + (1,), device=self.device))
+        return equilibrium_soa64(self.q, u, torch.ones(self.shape + (1,), device=self.device,
+                                                       dtype=dtype))
+
+    # -- FP64 storage ------------------------------------------------------------
+    # The float64 comparison run.  The per-function kernels are float32 only,
+    # so in this storage the state before the first step is kept with torch
+    # float64 operations, and entering the fused form applies LBMD3._init's
+    # collision and step 1's collision on the device (lbm_flow_init) in
+    # float64 to the initial field.
+    def _init_fp64(self):
+        X, Y, Z = self.shape
+        q, dev, dt = self.q, self.device, torch.float64
+        w = torch.tensor(VELOCITY_SETS[q][1], dtype=dt, device=dev)
+        self._f = w.reshape(q, 1).expand(q, self.n).contiguous()
+        self._f2 = None
+        self._feq = None
+        self._u = torch.zeros((X, Y, Z, 3), device=dev, dtype=dt)
+        self._rou = torch.ones((X, Y, Z, 1), device=dev, dtype=dt)
+        self._p = torch.zeros((X, Y, Z, 1), device=dev, dtype=dt)
+        self._FOL = torch.zeros((X, Y, Z, 3), device=dev, dtype=dt)
+        self._mode = "ref"
+        self._obs_valid = True
+        self._collisions = 0
+        self._moments64()
+        if self.config.init_field:
+            self._f = self.initial_field(self.config.init_field, dtype=dt)
+            self._moments64()
+
+    def _moments64(self):
+        """update_u_rou (flow/d3/base.py:116-133) in float64 torch operations."""
+        X, Y, Z = self.shape
+        e = torch.tensor(VELOCITY_SETS[self.q][0], dtype=torch.float64, device=self.device)
+        rou = self._f.sum(0).view(X, Y, Z, 1)
+        u = (e.t() @ self._f).t().reshape(X, Y, Z, 3)
+        u = (u + self._FOL / 2) / rou
+        for a in range(3):
+            for pl in (0, -1):
+                idx = [slice(None)] * 3
+                idx[a] = pl
+                u[tuple(idx)] = 0
+        self._rou, self._u, self._p = rou, u, rou / 3.0
+
+    def _fp64_only_fused(self, what):
+        raise NotImplementedError("%s: FP64 storage runs the fused path only" % what)
 
     # -- mode switches ---------------------------------------------------------
     def _to_ref(self):
@@ -250,12 +300,13 @@ class FlowD3(Flow):
         lat.observe(force, f=self._f, rho=self._rou, u=self._u)
         self._p = self._rou / 3.0
         new_field, new_uniform = fields
+        rdt = lat.real_dtype
+        # the uniform force reaches the kernels as float32
+        g = torch.tensor(new_uniform, device=self.device, dtype=torch.float32).to(rdt)
         if new_field is not None:
-            self._FOL = new_field.view(self.shape + (3,)) + torch.tensor(
-                new_uniform, device=self.device, dtype=torch.float32)
+            self._FOL = new_field.view(self.shape + (3,)) + g
         else:
-            self._FOL = torch.tensor(new_uniform, device=self.device, dtype=torch.float32).expand(
-                self.shape + (3,)).contiguous()
+            self._FOL = g.expand(self.shape + (3,)).contiguous()
         self._obs_valid = True
 
     def enter_fused(self):
@@ -267,6 +318,14 @@ class FlowD3(Flow):
         lat = self._lat
         if not lat.fused:
             raise NotImplementedError("NON_EQUILIBRIUM faces run in reference mode")
+        if self._fp64:
+            if self._collisions != 1 or bool(torch.any(self._FOL != 0)):
+                self._fp64_only_fused("entering the fused form from a stepped state")
+            lat.allocate()
+            lat.init(self._f)
+            self._mode = "fused"
+            self._obs_valid = False
+            return
         lat.allocate()
         post = self._f.clone()
         call("lbm_collide", ctypes_ref(lat.desc_fp32), ptr(post), ptr(self._rou), ptr(self._u),
@@ -299,6 +358,13 @@ class FlowD3(Flow):
     # -- reference methods (one kernel each) ---------------------------------
     def cul_equ(self, step=0, *args, **kwargs):
         """flow/d3/base.py:150-159"""
+        if getattr(self, "_fp64", False):
+            # LBMD3._init's collision, applied on the device when the fused
+            # form is entered
+            if self._mode != "ref" or self._collisions:
+                self._fp64_only_fused("cul_equ")
+            self._collisions = 1
+            return
         self._to_ref()
         if self._feq is None:
             self._feq = torch.empty_like(self._f)
@@ -307,6 +373,8 @@ class FlowD3(Flow):
 
     def f_stream(self, *args, **kwargs):
         """flow/d3/base.py:161-323"""
+        if getattr(self, "_fp64", False):
+            self._fp64_only_fused("f_stream")
         self._to_ref()
         if self._f2 is None:
             self._f2 = torch.empty_like(self._f)
@@ -319,6 +387,11 @@ class FlowD3(Flow):
 
     def update_u_rou(self, step=0, *args, **kwargs):
         """flow/d3/base.py:116-148"""
+        if getattr(self, "_fp64", False):
+            if self._mode != "ref" or self._collisions:
+                self._fp64_only_fused("update_u_rou")
+            self._moments64()
+            return
         self._to_ref()
         call("lbm_moments", ctypes_ref(self._lat.desc_fp32), ptr(self._f), ptr(self._FOL),
              ptr(self._rou), ptr(self._u), ptr(self._p), ptr(self._scratch), self._lat.stream())
@@ -329,6 +402,8 @@ class FlowD3(Flow):
 
     def cul_equ2(self, *args, **kwargs):
         """flow/d3/base.py:103-114"""
+        if getattr(self, "_fp64", False):
+            self._fp64_only_fused("cul_equ2")
         self._to_ref()
         call("lbm_add_force", ctypes_ref(self._lat.desc_fp32), ptr(self._f), ptr(self._u),
              ptr(self._FOL), self._lat.stream())
@@ -352,7 +427,8 @@ class FlowD3(Flow):
     def f(self, value):
         self._to_ref()
         X, Y, Z = self.shape
-        v = torch.as_tensor(value, dtype=torch.float32, device=self.device).reshape(X, Y, Z, self.q)
+        dt = torch.float64 if getattr(self, "_fp64", False) else torch.float32
+        v = torch.as_tensor(value, dtype=dt, device=self.device).reshape(X, Y, Z, self.q)
         self._f = v.permute(3, 0, 1, 2).contiguous().view(self.q, -1)
 
     @property
@@ -442,7 +518,7 @@ def face_planes(rho3):
     return torch.cat([p.reshape(-1) for p in parts])
 
 
-def taylor_green_velocity(shape, u0, device):
+def taylor_green_velocity(shape, u0, device, dtype=torch.float32):
     """u0 (sin kx cos ky cos kz, -cos kx sin ky cos kz, 0), k = 2 pi / N per axis."""
     X, Y, Z = shape
     kx, ky, kz = (2 * math.pi / s for s in (X, Y, Z))
@@ -452,7 +528,7 @@ def taylor_green_velocity(shape, u0, device):
     ux = u0 * torch.sin(kx * x) * torch.cos(ky * y) * torch.cos(kz * z)
     uy = -u0 * torch.cos(kx * x) * torch.sin(ky * y) * torch.cos(kz * z)
     uz = torch.zeros_like(ux * uy)
-    return torch.stack(torch.broadcast_tensors(ux, uy, uz), -1).to(torch.float32)
+    return torch.stack(torch.broadcast_tensors(ux, uy, uz), -1).to(dtype)
 
 
 def equilibrium_soa(param, u, rou):
@@ -462,6 +538,18 @@ def equilibrium_soa(param, u, rou):
     u2 = torch.linalg.norm(u, dim=-1, keepdim=True) ** 2 / cs2 / 2
     feq = (1 + tmp + tmp ** 2 / 2 - u2) * torch.matmul(rou, param.w)
     return feq.reshape(-1, param.e_dim).t().contiguous()
+
+
+def equilibrium_soa64(q, u, rou):
+    """feq of flow/d3/base.py:152-158 in float64 with cs^2 = 1/3 (the FP64
+    comparison run), SoA [Q, n]."""
+    e = torch.tensor(VELOCITY_SETS[q][0], dtype=torch.float64, device=u.device)
+    w = torch.tensor([VELOCITY_SETS[q][1]], dtype=torch.float64, device=u.device)
+    cs2 = math.sqrt(1.0 / 3) ** 2
+    tmp = torch.matmul(u, e.t()) / cs2
+    u2 = torch.linalg.norm(u, dim=-1, keepdim=True) ** 2 / cs2 / 2
+    feq = (1 + tmp + tmp ** 2 / 2 - u2) * torch.matmul(rou, w)
+    return feq.reshape(-1, q).t().contiguous()
 
 
 class FlowD3Q13(FlowD3):

@@ -17,8 +17,13 @@ from . import _lib
 from ._lib import LbmForce, LbmLattice, LbmObserve, call, ptr
 
 BC = {"PERIODICAL": 11000, "WALL": 1200, "WALL_WITH_SPEED": 1201, "NON_EQUILIBRIUM": 1400}
-STORAGE_DTYPE = {"fp32": torch.float32, "fp16s": torch.float16, "bf16s": torch.bfloat16}
-BYTES = {"fp32": 4, "fp16s": 2, "bf16s": 2}
+STORAGE_DTYPE = {"fp32": torch.float32, "fp16s": torch.float16, "bf16s": torch.bfloat16,
+                 "fp64": torch.float64}
+BYTES = {"fp32": 4, "fp16s": 2, "bf16s": 2, "fp64": 8}
+# arithmetic type of a storage: what its fields, face densities, force fields
+# and observation buffers hold
+REAL_DTYPE = {"fp32": torch.float32, "fp16s": torch.float32, "bf16s": torch.float32,
+              "fp64": torch.float64}
 
 
 def cs2_float32():
@@ -103,7 +108,7 @@ class Lattice:
     def bytes_needed(q, shape, storage="fp32"):
         n = int(shape[0]) * int(shape[1]) * int(shape[2])
         planes = 2 * (shape[1] * shape[2] + shape[0] * shape[2] + shape[0] * shape[1])
-        return 2 * q * n * BYTES[storage] + 2 * 4 * planes
+        return 2 * q * n * BYTES[storage] + 2 * REAL_DTYPE[storage].itemsize * planes
 
     def allocate(self):
         dt = STORAGE_DTYPE[self.storage]
@@ -112,8 +117,8 @@ class Lattice:
                 self.buf[i] = torch.empty(self.q * self.n, dtype=dt, device=self.device)
         if self.needs_face_rho and self.face_rho[0] is None:
             nplanes = _lib.load().lbm_face_plane_floats(ctypes_ref(self.desc))
-            self.face_rho = [torch.zeros(nplanes, dtype=torch.float32, device=self.device)
-                             for _ in range(2)]
+            self.face_rho = [torch.zeros(nplanes, dtype=REAL_DTYPE[self.storage],
+                                         device=self.device) for _ in range(2)]
         if self.status is None:
             self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
 
@@ -125,14 +130,22 @@ class Lattice:
     def stream(self):
         return _lib.stream_of(torch, self.device)
 
+    @property
+    def real_dtype(self):
+        return REAL_DTYPE[self.storage]
+
     def init(self, f0=None):
-        """Post-collision populations of step 1 from f0 (float32 SoA) or rho*w."""
+        """Post-collision populations of step 1 from f0 (SoA in the storage's
+        arithmetic type: float64 for fp64, float32 otherwise) or rho*w."""
+        if f0 is not None and f0.dtype != self.real_dtype:
+            raise TypeError("initial field of a %s lattice must be %s" % (self.storage,
+                                                                          self.real_dtype))
         call("lbm_flow_init", ctypes_ref(self.desc), ptr(f0), ptr(self.buf[self.cur]),
              ptr(self.face_rho[self.cur]), self.stream())
 
     def load_post_collision_fp32(self, a):
         """Adopt float32 SoA post-collision populations (storage conversion on device)."""
-        if self.storage == "fp32":
+        if self.storage in ("fp32", "fp64"):
             self.buf[self.cur].copy_(a.reshape(-1))
         else:
             w = weights_tensor(self.q, self.device)

@@ -106,8 +106,9 @@ class LBMBase:
         self.device = _device_of(self.config)
         self.step = 1
         self.flow = flow or create_flow(flow_config=self.config.flow_config, device=self.device)
-        self.particle_swarm = particle_swarm or create_particle_swarm(self.config.particles,
-                                                                      device=self.device)
+        pdt = torch.float64 if self.config.flow_config.storage == "fp64" else torch.float32
+        self.particle_swarm = particle_swarm or create_particle_swarm(
+            self.config.particles, device=self.device, dtype=pdt)
         self.run_status = True
         self.status_word = 0
         self._g_old = (0.0, 0.0, 0.0)
@@ -387,7 +388,8 @@ class LBMD3(LBMBase):
             return
         n = self.flow.n
         dev = self.device
-        self._fol = [torch.zeros(n * 3, device=dev) for _ in range(2)]
+        rdt = self.flow.lattice.real_dtype
+        self._fol = [torch.zeros(n * 3, device=dev, dtype=rdt) for _ in range(2)]
         nch = (n + 31) // 32
         self._chunks = [torch.zeros(nch, dtype=torch.uint8, device=dev) for _ in range(2)]
         self._owner = torch.full((n,), -1, dtype=torch.int32, device=dev)

@@ -130,12 +130,13 @@ class Coordinate:
     """Body frame of a particle (particle/coord.py:46-120).  ``angle`` is the
     accumulated rotation vector; ``center`` the centre of mass."""
 
-    def __init__(self, config: CoordConfig = None, device="cuda", *args, **kwargs):
+    def __init__(self, config: CoordConfig = None, device="cuda", dtype=torch.float32, *args,
+                 **kwargs):
         config = config or CoordConfig()
         self.device = _device(device)
-        self._center = torch.tensor(config.center, device=self.device, dtype=torch.float32)
+        self._center = torch.tensor(config.center, device=self.device, dtype=dtype)
         self._angle = torch.tensor([config.alpha, config.beta, config.gamma], device=self.device,
-                                   dtype=torch.float32)
+                                   dtype=dtype)
 
     @property
     def center(self):
@@ -143,7 +144,7 @@ class Coordinate:
 
     @center.setter
     def center(self, v):
-        self._center.copy_(torch.as_tensor(v, dtype=torch.float32))
+        self._center.copy_(torch.as_tensor(v, dtype=self._center.dtype))
 
     @property
     def angle(self):
@@ -151,7 +152,7 @@ class Coordinate:
 
     @angle.setter
     def angle(self, v):
-        self._angle.copy_(torch.as_tensor(v, dtype=torch.float32))
+        self._angle.copy_(torch.as_tensor(v, dtype=self._angle.dtype))
 
     @property
     def rotation(self):
@@ -162,7 +163,7 @@ class Coordinate:
         pts = np.asarray(points.detach().cpu().numpy() if isinstance(points, torch.Tensor) else points,
                          np.float64)
         rot = pts @ self.rotation.T
-        return torch.tensor(rot, device=self.device, dtype=torch.float32) + self._center
+        return torch.tensor(rot, device=self.device, dtype=self._center.dtype) + self._center
 
     def update(self, center, w):
         self.center = center
@@ -199,25 +200,29 @@ _MARKER = ("lx", "lF", "lu", "lm", "lrou", "_lagrange")
 
 class Particle:
     """Rigid particle (particle/base/base.py:22-214).  Before the swarm packs
-    it the state lives in its own tensors; afterwards in the swarm arrays."""
+    it the state lives in its own tensors; afterwards in the swarm arrays.
+    ``dtype`` is float32 (the reference's) or float64 (particles of an FP64
+    lattice)."""
 
-    def __init__(self, config: ParticleConfig = None, device="cuda", *args, **kwargs):
+    def __init__(self, config: ParticleConfig = None, device="cuda", dtype=torch.float32, *args,
+                 **kwargs):
         self.device = _device(device)
+        self.dtype = dtype
         self.config = config or ParticleConfig()
-        self.coord = Coordinate(config=self.config.coord_config, device=self.device)
+        self.coord = Coordinate(config=self.config.coord_config, device=self.device, dtype=dtype)
         self.mass = None
         self.area = None
         self.I = None
         self.rou = None
         self._t = {
-            "cx": torch.tensor(self.config.coord_config.center, device=self.device, dtype=torch.float32),
-            "cu": torch.zeros(3, device=self.device),
-            "cw": torch.zeros(3, device=self.device),
-            "cF": torch.zeros(3, device=self.device),
-            "cT": torch.zeros(3, device=self.device),
+            "cx": torch.tensor(self.config.coord_config.center, device=self.device, dtype=dtype),
+            "cu": torch.zeros(3, device=self.device, dtype=dtype),
+            "cw": torch.zeros(3, device=self.device, dtype=dtype),
+            "cF": torch.zeros(3, device=self.device, dtype=dtype),
+            "cT": torch.zeros(3, device=self.device, dtype=dtype),
         }
         for k in _MARKER:
-            self._t[k] = torch.zeros([0], device=self.device)
+            self._t[k] = torch.zeros([0], device=self.device, dtype=dtype)
         self._swarm = None
         self._index = None
 
@@ -230,13 +235,14 @@ class Particle:
         self.rou = float(self.config.get("rou", 1.0))
         self._init(*args, **kwargs)
         n = self._t["_lagrange"].shape[0]
-        self._t["lx"] = torch.zeros((n, 3), device=self.device)
-        self._t["lF"] = torch.zeros((n, 3), device=self.device)
-        self._t["lu"] = torch.zeros((n, 3), device=self.device)
-        # lm = area / N as a float32 tensor division, like torch.full((N, 1), area / N)
+        dt = self.dtype
+        self._t["lx"] = torch.zeros((n, 3), device=self.device, dtype=dt)
+        self._t["lF"] = torch.zeros((n, 3), device=self.device, dtype=dt)
+        self._t["lu"] = torch.zeros((n, 3), device=self.device, dtype=dt)
+        # lm = area / N as a tensor division, like torch.full((N, 1), area / N)
         self._t["lm"] = ((self.area / n).reshape(1, 1).expand(n, 1).contiguous() if n
-                         else torch.zeros((0, 1), device=self.device))
-        self._t["lrou"] = torch.zeros((n, 1), device=self.device)
+                         else torch.zeros((0, 1), device=self.device, dtype=dt))
+        self._t["lrou"] = torch.zeros((n, 1), device=self.device, dtype=dt)
 
     # attribute views ---------------------------------------------------------
     def _view(self, key):
@@ -250,7 +256,7 @@ class Particle:
     def __setattr__(self, key, value):
         if key in _STATE or key in _MARKER:
             t = self.__dict__["_t"][key]
-            v = torch.as_tensor(value, dtype=torch.float32, device=t.device)
+            v = torch.as_tensor(value, dtype=t.dtype, device=t.device)
             if t.numel() == v.numel() and t.numel() > 0:
                 t.copy_(v.reshape(t.shape))
             else:
@@ -318,7 +324,7 @@ class Particle:
 _MARKER_CACHE = {}
 
 
-def _markers_tensor(ra, rb, rc, dx, device):
+def _markers_tensor(ra, rb, rc, dx, device, dtype=torch.float32):
     """Body-frame markers of an ellipsoid (a sphere when ra = rb = rc); the
     generator is deterministic, so each shape is computed once per process."""
     key = (float(ra), float(rb), float(rc), float(dx))
@@ -327,7 +333,7 @@ def _markers_tensor(ra, rb, rc, dx, device):
             -ra - 2 * dx, -rb - 2 * dx, -rc - 2 * dx, ra + 2 * dx, rb + 2 * dx, rc + 2 * dx,
             dx=dx, semi_axes=(ra, rb, rc))
     pts = _MARKER_CACHE[key]
-    return torch.tensor(pts, device=device, dtype=torch.float32).reshape(-1, 3)
+    return torch.tensor(pts, device=device, dtype=dtype).reshape(-1, 3)
 
 
 class Sphere(Particle):
@@ -339,11 +345,12 @@ class Sphere(Particle):
 
     def _init(self, dx=1, *args, **kwargs):
         r = self.r
-        self._t["_lagrange"] = _markers_tensor(r, r, r, dx, self.device)
-        self.mass = torch.tensor(4.0 / 3.0 * math.pi * r * r * r, device=self.device, dtype=torch.float32)
-        self.area = torch.tensor(4.0 * math.pi * r * r, device=self.device, dtype=torch.float32)
+        dt = self.dtype
+        self._t["_lagrange"] = _markers_tensor(r, r, r, dx, self.device, dt)
+        self.mass = torch.tensor(4.0 / 3.0 * math.pi * r * r * r, device=self.device, dtype=dt)
+        self.area = torch.tensor(4.0 * math.pi * r * r, device=self.device, dtype=dt)
         self.I = torch.tensor(np.array([r * r, r * r, r * r]) * self.mass.cpu().numpy() / 5.0,
-                              device=self.device, dtype=torch.float32)
+                              device=self.device, dtype=dt)
 
 
 class Ellipsoid(Particle):
@@ -357,32 +364,36 @@ class Ellipsoid(Particle):
 
     def _init(self, dx=1, *args, **kwargs):
         a, b, c = self.ra, self.rb, self.rc
-        self._t["_lagrange"] = _markers_tensor(a, b, c, dx, self.device)
-        self.mass = torch.tensor(4.0 / 3.0 * math.pi * a * b * c, device=self.device, dtype=torch.float32)
+        dt = self.dtype
+        self._t["_lagrange"] = _markers_tensor(a, b, c, dx, self.device, dt)
+        self.mass = torch.tensor(4.0 / 3.0 * math.pi * a * b * c, device=self.device, dtype=dt)
         self.area = torch.tensor(4.0 / 3.0 * math.pi * math.pow(a * b * c, 2.0 / 3.0),
-                                 device=self.device, dtype=torch.float32)
+                                 device=self.device, dtype=dt)
         self.I = torch.tensor(np.array([b * c, a * c, a * b]) * self.mass.cpu().numpy() / 5.0,
-                              device=self.device, dtype=torch.float32)
+                              device=self.device, dtype=dt)
 
 
-def create_particle(config: ParticleConfig, device="cuda") -> Particle:
+def create_particle(config: ParticleConfig, device="cuda", dtype=torch.float32) -> Particle:
     """particle/base/__init__.py:8-12"""
     if config.type == "ellipsoid":
-        return Ellipsoid(config=config, device=device)
-    return Sphere(config=config, device=device)
+        return Ellipsoid(config=config, device=device, dtype=dtype)
+    return Sphere(config=config, device=device, dtype=dtype)
 
 
 class ParticleSwarm:
     """particle/swarm.py:12-41, with the device arrays of all particles."""
 
-    def __init__(self, configs: List[ParticleConfig] = (), device="cuda"):
+    def __init__(self, configs: List[ParticleConfig] = (), device="cuda", dtype=torch.float32):
         self.device = _device(device)
-        self.particles: List[Particle] = [create_particle(c, device=self.device) for c in configs]
+        self.dtype = dtype
+        self.particles: List[Particle] = [create_particle(c, device=self.device, dtype=dtype)
+                                          for c in configs]
         self._packed = False
 
     @classmethod
     def adopt(cls, particles, device):
-        sw = cls((), device)
+        dtype = particles[0].dtype if particles else torch.float32
+        sw = cls((), device, dtype=dtype)
         sw.particles = list(particles)
         sw.pack()
         return sw
@@ -409,10 +420,12 @@ class ParticleSwarm:
         M = int(offs[-1])
         P = len(ps)
 
+        dt = self.dtype
+
         def cat_markers(key, width):
             if M == 0:
-                return torch.zeros((0, width), device=dev)
-            return torch.cat([p._t[key].reshape(-1, width) for p in ps]).contiguous()
+                return torch.zeros((0, width), device=dev, dtype=dt)
+            return torch.cat([p._t[key].reshape(-1, width).to(dt) for p in ps]).contiguous()
 
         self.lagrange = cat_markers("_lagrange", 3)
         self.lx = cat_markers("lx", 3)
@@ -422,15 +435,16 @@ class ParticleSwarm:
         self.lrou = cat_markers("lrou", 1)
 
         def stack(key):
-            return (torch.stack([p._t[key] for p in ps]).contiguous() if P
-                    else torch.zeros((0, 3), device=dev))
+            return (torch.stack([p._t[key].to(dt) for p in ps]).contiguous() if P
+                    else torch.zeros((0, 3), device=dev, dtype=dt))
 
         self.cx, self.cu, self.cw, self.cF, self.cT = (stack(k) for k in _STATE)
-        self.angle = (torch.stack([p.coord.angle for p in ps]).contiguous() if P
-                      else torch.zeros((0, 3), device=dev))
-        self.mass = torch.tensor([float(p.mass) for p in ps], dtype=torch.float32, device=dev)
-        self.inertia = (torch.stack([p.I for p in ps]).contiguous() if P else torch.zeros((0, 3), device=dev))
-        self.rou = torch.tensor([float(p.rou) for p in ps], dtype=torch.float32, device=dev)
+        self.angle = (torch.stack([p.coord.angle.to(dt) for p in ps]).contiguous() if P
+                      else torch.zeros((0, 3), device=dev, dtype=dt))
+        self.mass = torch.tensor([float(p.mass) for p in ps], dtype=dt, device=dev)
+        self.inertia = (torch.stack([p.I.to(dt) for p in ps]).contiguous() if P
+                        else torch.zeros((0, 3), device=dev, dtype=dt))
+        self.rou = torch.tensor([float(p.rou) for p in ps], dtype=dt, device=dev)
         for i, p in enumerate(ps):
             a, b = int(offs[i]), int(offs[i + 1])
             for key, arr in (("_lagrange", self.lagrange), ("lx", self.lx), ("lF", self.lF),
@@ -468,6 +482,7 @@ class ParticleSwarm:
         s.mass = at(self.mass, p0)
         s.inertia = at(self.inertia, p0)
         s.rou = at(self.rou, p0)
+        s.fp64 = 1 if self.dtype == torch.float64 else 0
         return s
 
     def struct(self):
@@ -506,5 +521,6 @@ class ParticleSwarm:
             particle.load_checkpoint(group.get("particle_%06d" % i), *args, **kwargs)
 
 
-def create_particle_swarm(configs: List[ParticleConfig] = (), device="cuda", *args, **kwargs):
-    return ParticleSwarm(configs=configs, device=device)
+def create_particle_swarm(configs: List[ParticleConfig] = (), device="cuda", dtype=torch.float32,
+                          *args, **kwargs):
+    return ParticleSwarm(configs=configs, device=device, dtype=dtype)

@@ -18,7 +18,9 @@ ROWS = -1   # whole z-rows staged in shared memory by TMA bulk copies
 CANDIDATES = {
     32: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256), (ROWS, 256)],
     16: [(1, 256), (2, 128), (2, 256), (4, 128), (4, 256), (8, 128), (8, 256), (ROWS, 256)],
+    64: [(1, 256), (2, 128), (2, 256)],
 }
+STORAGE_BITS = {"fp32": 32, "fp16s": 16, "bf16s": 16, "fp64": 64}
 _CACHE = {}
 PROXY_BYTES = 2 << 30          # populations of the proxy lattice (both buffers)
 
@@ -27,7 +29,7 @@ def shape_ok(nodes, nz, bits):
     if nodes == 1:
         return True
     if nodes == ROWS:
-        return (nz * bits // 8) % 16 == 0 and nz >= 16
+        return bits != 64 and (nz * bits // 8) % 16 == 0 and nz >= 16
     if nodes * bits // 32 not in (1, 2, 4):
         return False
     if nodes == 2 and bits == 16 and nz % 2 == 1 and nz >= 3:
@@ -39,7 +41,7 @@ def default_shape(q, storage, nz, forced=False):
     """The launch shape lbm_flow_step uses when none is set (measured best at
     512^3): 2 nodes per thread with 128 threads, 4 for unforced D3Q19 in
     16-bit storage, one node per thread where rows allow no vector."""
-    bits = 32 if storage == "fp32" else 16
+    bits = STORAGE_BITS[storage]
     want = 4 if (bits == 16 and q == 19 and not forced) else 2
     for nodes in (want, 2):
         if nz % nodes == 0 and nz >= 2 * nodes:
@@ -65,7 +67,7 @@ def tune(lat, force=None, iters=6, warmup=2, verbose=False):
     in its descriptor.  Returns the choice and the timings in ms per step."""
     from .lattice import BYTES, Lattice
 
-    bits = 32 if lat.storage == "fp32" else 16
+    bits = STORAGE_BITS[lat.storage]
     key = (lat.q, lat.storage, lat.shape[1], lat.shape[2], force is not None)
     if key in _CACHE:
         choice, timings = _CACHE[key]
@@ -148,7 +150,7 @@ def tune_class_of(q, storage, nz, forced, device="cuda", iters=6, warmup=2):
         field *= flags.repeat_interleave(32)[:pn, None].to(field.dtype)
         keep = [field.reshape(-1), flags]
         force = make_force((0, 0, 0), (0, 0, 0), keep[0], keep[0], keep[1], keep[1])
-    bits = 32 if storage == "fp32" else 16
+    bits = STORAGE_BITS[storage]
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     timings = {}

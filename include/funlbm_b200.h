@@ -60,6 +60,12 @@ extern "C" {
 #define LBM_STORAGE_FP32 0  /* float32 populations (the reference's type)       */
 #define LBM_STORAGE_FP16S 1 /* float16 of (f_i - w_i), collided in float32       */
 #define LBM_STORAGE_BF16S 2 /* bfloat16 of (f_i - w_i), collided in float32      */
+#define LBM_STORAGE_FP64 3  /* float64 populations and float64 arithmetic: the  */
+                            /* comparison run of the storage error figures (the */
+                            /* reference itself is float32 only).  Every float  */
+                            /* buffer of a call on such a lattice -- initial    */
+                            /* field, force fields, face densities, observed    */
+                            /* f / rho / u, particle arrays -- holds float64.   */
 
 #define LBM_STEP_ROWS (-1)
 
@@ -205,6 +211,8 @@ typedef struct lbm_particles {
   const float *mass;             /* [n_particles]                             */
   const float *inertia;          /* [n_particles][3]                          */
   const float *rou;              /* [n_particles] particle density            */
+  int32_t fp64;                  /* 1: every float array above holds float64  */
+                                 /* (particles of an LBM_STORAGE_FP64 lattice) */
 } lbm_particles;
 
 /* LBMD3.flow_to_lagrange (lbm/lbm3d.py:66-100) fused with the moment pass

@@ -119,7 +119,7 @@ class OracleFlow:
     FOL[X,Y,Z,3], with X,Y,Z = size+1 (flow/d3/base.py:81-82).
     """
 
-    def __init__(self, q, size, mu, faces=None, face_uw=None, Re=10.0, dtype=np.float32):
+    def __init__(self, q, size, mu, faces=None, face_uw=None, Re=10.0, dtype=np.float32, tau=None):
         self.q = q
         self.dtype = dtype
         e, w, rev = velocity_set(q)
@@ -142,7 +142,9 @@ class OracleFlow:
         self.face_uw = {k: np.asarray((face_uw or {}).get(k, (0.0, 0.0, 0.0)), dtype=dtype)
                         for k in FACES}
         self.cs2 = cs2_of(dtype)
-        self.tau = dtype(3 * self.mu + 0.5)          # flow/d3/base.py:96
+        # flow/d3/base.py:96; `tau` overrides it (an FP64 run with the float32
+        # relaxation time of the run it is compared with)
+        self.tau = dtype(3 * self.mu + 0.5) if tau is None else dtype(tau)
         self._profile = None
 
     # -- flow/d3/base.py:72-101 ------------------------------------------

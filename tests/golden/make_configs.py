@@ -2,6 +2,7 @@
 running the reference funlbm 1.2.0 itself on the CPU.
 
     python tests/golden/make_configs.py --reference <funlbm checkout>/src [--only config1|config2]
+                                        [--device cuda]
 
 (or set FUNLBM_REFERENCE_SRC instead of --reference).  Like ``make_golden.py``
 it puts the project-written stand-ins of ``tests/golden/_stubs`` in front of
@@ -13,7 +14,12 @@ the reference for its five absent helper packages.
   u = 0, 2000 steps.  The reference has no body-force option; the script adds
   the force to FOL right after ``lagrange_to_flow`` (lbm/lbm3d.py:102-119)
   resets it, which is where this build's ``flow.body_force`` extension and
-  the oracle apply it.  Recorded: rho and u after steps 1000 and 2000.
+  the oracle apply it.  Recorded: rho and u after steps 1000 and 2000.  The
+  same file carries the float64 run of the oracle (``oracle/lbm_oracle.py``)
+  of this configuration -- rho and u on the mid plane z = 32 and the mean
+  density after steps 1000 and 2000 -- the yardstick of float32 rounding: the
+  reference's float32 run drifts from it by ~2.5e-5 in rho (its total mass
+  grows) and ~1.4e-2 of max|u| in u over 2000 steps.
 * ``config2_sphere.npz`` -- the single-sphere free fall in the reference's
   axes (gravity acts along +x scaled by 1 - rho_p / rho_f, so the fall is
   along -x): D3Q19, size [160, 64, 64] (161 x 65 x 65 nodes), every face
@@ -22,8 +28,14 @@ the reference for its five absent helper packages.
   particle's cx, cu, cw, cF and rotation vector after every step, and rho /
   u on the mid plane z = 32 at the end.
 
-CPU time: about a minute for config 1 and about an hour for config 2 (the
-reference's interpolation and spreading are Python loops over the markers).
+CPU time: a few minutes for config 1 and one to several hours for config 2
+(the reference's interpolation and spreading are Python loops over the
+markers).  ``--device cuda`` runs the reference's own torch code with its
+flow and particles on the GPU instead (created by its ``create_flow`` /
+``create_particle_swarm`` and handed to ``LBMD3``, which otherwise always
+builds them on the CPU: lbm/base.py:56-76, base/work.py:41-43); the
+installed copy in baseline/_ref serves as ``--reference`` where the source
+tree is not mounted.  The device is recorded in the fixture.
 Nothing here runs at test time; the tests only read the ``.npz`` files.
 """
 from __future__ import annotations
@@ -51,16 +63,21 @@ def _setup(ref_src):
     sys.path.insert(0, ref_src)
 
 
-def _lbm(q, size, mu, faces, particles=(), gl=0.0):
+def _lbm(q, size, mu, faces, particles=(), gl=0.0, device="cpu"):
+    from funlbm.flow import create_flow
     from funlbm.lbm import LBMD3, Config
+    from funlbm.particle import create_particle_swarm
 
     cfg = Config().from_json({
-        "device": "cpu", "dt": 1, "dx": 1,
+        "device": device, "dt": 1, "dx": 1,
         "flow": {"size": list(size), "param_type": "D3Q%d" % q, "param": {"mu": mu, "gl": gl},
                  "boundary": {k: {"code": v} for k, v in zip(FACES, faces)}},
         "particles": list(particles), "file": {"per_steps": 10 ** 9},
     })
-    return LBMD3(config=cfg)
+    if device == "cpu":
+        return LBMD3(config=cfg)
+    return LBMD3(config=cfg, flow=create_flow(cfg.flow_config, device=device),
+                 particle_swarm=create_particle_swarm(cfg.particles, device=device), device=device)
 
 
 def make_config1():
@@ -90,10 +107,35 @@ def make_config1():
     return out
 
 
-def make_config2(steps=None):
+def make_config1_oracle64():
+    """The float64 oracle run of config 1 (mid-plane rho / u, mean rho)."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle import lbm_oracle as O
+
+    c = CONFIG1
+    code = {"WALL": O.WALL, "PERIODICAL": O.PERIODICAL}
+    fl = O.OracleFlow(19, c["size"], c["mu"], dict(zip(O.FACES, [code[v] for v in c["faces"]])),
+                      dtype=np.float64)
+    lbm = O.OracleLBM(fl, body_force=c["body_force"])
+    lbm.init(None)
+    out = {}
+    zmid = c["size"][2] // 2
+    t0 = time.time()
+    for s in range(1, c["steps"] + 1):
+        lbm.run_step()
+        lbm.step += 1
+        if s in c["record"]:
+            out["oracle64_rou_mid_%d" % s] = fl.rou[:, :, zmid].copy()
+            out["oracle64_u_mid_%d" % s] = fl.u[:, :, zmid].copy()
+            out["oracle64_rou_mean_%d" % s] = np.float64(fl.rou.mean())
+    print("config1 oracle float64: %d steps in %.1f s" % (c["steps"], time.time() - t0), flush=True)
+    return out
+
+
+def make_config2(steps=None, device="cpu"):
     c = CONFIG2
     steps = c["steps"] if steps is None else steps
-    lbm = _lbm(19, c["size"], c["mu"], ("WALL",) * 6, [c["particle"]], gl=c["gl"])
+    lbm = _lbm(19, c["size"], c["mu"], ("WALL",) * 6, [c["particle"]], gl=c["gl"], device=device)
     lbm.init()
     p = lbm.particle_swarm.particles[0]
     hist = {k: [] for k in ("cx", "cu", "cw", "cF", "angle")}
@@ -101,7 +143,7 @@ def make_config2(steps=None):
     for s in range(steps):
         lbm.run_step(step=lbm.step)
         for k in hist:
-            hist[k].append((p.coord.angle if k == "angle" else getattr(p, k)).numpy().copy())
+            hist[k].append((p.coord.angle if k == "angle" else getattr(p, k)).cpu().numpy().copy())
         if not lbm.run_status:
             raise RuntimeError("the reference stopped its run at step %d" % lbm.step)
         lbm.step += 1
@@ -110,10 +152,11 @@ def make_config2(steps=None):
                   flush=True)
     out = {k: np.stack(v).astype(np.float32) for k, v in hist.items()}
     zmid = c["size"][2] // 2
-    out["rou_mid"] = lbm.flow.rou[:, :, zmid].numpy().copy()
-    out["u_mid"] = lbm.flow.u[:, :, zmid].numpy().copy()
-    out["lagrange"] = p._lagrange.numpy().copy()
+    out["rou_mid"] = lbm.flow.rou[:, :, zmid].cpu().numpy().copy()
+    out["u_mid"] = lbm.flow.u[:, :, zmid].cpu().numpy().copy()
+    out["lagrange"] = p._lagrange.cpu().numpy().copy()
     out["steps"] = np.int32(steps)
+    out["device"] = np.array(str(device))
     return out
 
 
@@ -125,6 +168,7 @@ def main():
     ap.add_argument("--only", choices=["config1", "config2"], default=None)
     ap.add_argument("--config2-steps", type=int, default=None)
     ap.add_argument("--threads", type=int, default=os.cpu_count())
+    ap.add_argument("--device", default="cpu", help="config 2 only: cpu or cuda")
     args = ap.parse_args()
     if not args.reference:
         ap.error("pass --reference or set FUNLBM_REFERENCE_SRC")
@@ -137,11 +181,12 @@ def main():
         os.chdir(tmp)
         try:
             if args.only in (None, "config1"):
-                np.savez_compressed(os.path.join(args.out, "config1_poiseuille.npz"),
-                                    **make_config1())
+                out = make_config1()
+                out.update(make_config1_oracle64())
+                np.savez_compressed(os.path.join(args.out, "config1_poiseuille.npz"), **out)
             if args.only in (None, "config2"):
                 np.savez_compressed(os.path.join(args.out, "config2_sphere.npz"),
-                                    **make_config2(args.config2_steps))
+                                    **make_config2(args.config2_steps, args.device))
         finally:
             os.chdir(cwd)
 
