@@ -103,6 +103,7 @@ SIGNATURES = {
     "lbm_lattice_check": (I, [_LAT]),
     "lbm_flow_init": (I, [_LAT, _P, _P, _P, _P]),
     "lbm_flow_step": (I, [_LAT, _P, _P, _FORCE, _P, _P, _OBS, _P, _P]),
+    "lbm_flow_stats": (I, [_LAT, _P, _FORCE, _P, _P, _P, _P]),
     "lbm_batch_entry_bytes": (ctypes.c_size_t, []),
     "lbm_batch_pack": (I, [_LAT, _P, _P, _FORCE, _P, _P, _P, ctypes.c_int32, _P, _P]),
     "lbm_flow_step_batch": (I, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -8,7 +8,8 @@ namespace lbm {
 #define LBM_EXTERN_STEP(Q, S)                                                                 \
   extern template int run_step_qs<Q, S>(const StepArgs &, bool, int, int, cudaStream_t);      \
   extern template int run_step_batch_qs<Q, S>(const StepArgs *, const unsigned *, int, unsigned, \
-                                              bool, int, cudaStream_t);
+                                              bool, int, cudaStream_t);                      \
+  extern template int run_stats_qs<Q, S>(const StepArgs &, bool, unsigned long long *, cudaStream_t);
 LBM_FOR_EACH_QS(LBM_EXTERN_STEP)
 #undef LBM_EXTERN_STEP
 
@@ -377,6 +378,27 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
   }
   return run_step(a, lat->q, lat->storage, use_force, (int)lat->step_nodes,
                   (int)lat->step_threads, (cudaStream_t)stream);
+}
+
+int lbm_flow_stats(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                   const float *face_rho_in, double *out, uint32_t *status, void *stream) {
+  if (out == nullptr) {
+    set_error("lbm_flow_stats: needs an output buffer of 9 doubles");
+    return LBM_ERR_INVALID;
+  }
+  StepArgs a;
+  bool use_force = false;
+  int rc = build_step_args(lat, fa, nullptr, force, face_rho_in, nullptr, nullptr, status, a,
+                           use_force, "lbm_flow_stats");
+  if (rc) return rc;
+  unsigned long long *slots = reinterpret_cast<unsigned long long *>(out);
+  cudaStream_t s = (cudaStream_t)stream;
+#define LBM_CASE_STATS(Q, S) \
+  if (lat->q == Q && lat->storage == S) return run_stats_qs<Q, S>(a, use_force, slots, s);
+  LBM_FOR_EACH_QS(LBM_CASE_STATS)
+#undef LBM_CASE_STATS
+  set_error("Unknown parameter type: D3Q%d", lat->q);
+  return LBM_ERR_INVALID;
 }
 
 size_t lbm_batch_entry_bytes(void) { return sizeof(StepArgs); }

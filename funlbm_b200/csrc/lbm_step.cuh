@@ -72,10 +72,13 @@ __device__ __forceinline__ ChunkForce chunk_force(const StepArgs &a, unsigned id
   return c;
 }
 
+// finish_node_m also hands the node's end-of-step moments (the second
+// update_u_rou) to the caller.
 template <int Q, bool FORCE, bool DEV, typename R>
-__device__ __forceinline__ void finish_node(const StepArgs &a, R f[Q], unsigned idx, int x,
-                                            int y, int z, bool face, ChunkForce cf,
-                                            unsigned &bad) {
+__device__ __forceinline__ void finish_node_m(const StepArgs &a, R f[Q], unsigned idx, int x,
+                                              int y, int z, bool face, ChunkForce cf,
+                                              unsigned &bad, R &rho_out, R &ux_out, R &uy_out,
+                                              R &uz_out) {
   using V = VSet<Q>;
   R fox = a.go[0], foy = a.go[1], foz = a.go[2];
   R fnx = a.gn[0], fny = a.gn[1], fnz = a.gn[2];
@@ -126,12 +129,24 @@ __device__ __forceinline__ void finish_node(const StepArgs &a, R f[Q], unsigned 
     ou[3ull * idx + 1] = uy;
     ou[3ull * idx + 2] = uz;
   }
+  rho_out = rho;
+  ux_out = ux;
+  uy_out = uy;
+  uz_out = uz;
   if (a.fb != nullptr) {
     if constexpr (DEV)
       collide_dev<Q>(f, a.g, rho, drho, ux, uy, uz);
     else
       collide<Q>(f, a.g, rho, ux, uy, uz);
   }
+}
+
+template <int Q, bool FORCE, bool DEV, typename R>
+__device__ __forceinline__ void finish_node(const StepArgs &a, R f[Q], unsigned idx, int x,
+                                            int y, int z, bool face, ChunkForce cf,
+                                            unsigned &bad) {
+  R rho, ux, uy, uz;
+  finish_node_m<Q, FORCE, DEV>(a, f, idx, x, y, z, face, cf, bad, rho, ux, uy, uz);
 }
 
 __device__ __forceinline__ void report_bad(unsigned *status, unsigned bad) {
@@ -183,6 +198,135 @@ constexpr int scalar_min_blocks() {
 template <int Q, int S, bool FORCE>
 __global__ void __launch_bounds__(kThreads, (scalar_min_blocks<Q, S>())) k_step(const StepArgs a) {
   step_scalar_body<Q, S, FORCE>(a, blockIdx.x * kThreads + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Step statistics: min / sum / max of f, u and rho at the end of the step the
+// populations `fa` stream into (FlowD3.to_json, flow/base.py:183-206, as
+// LBMBase._log_step_info logs it, lbm/base.py:105-144), in one read of the
+// populations and nothing written but 9 numbers.  Grid-stride, one node per
+// thread per iteration; per-block reduction, then one atomic per quantity
+// and block into `out`: min / max as order-preserving 64-bit keys of the
+// doubles, sums as doubles (k_stats_finish turns them into min, mean, max).
+// ---------------------------------------------------------------------------
+constexpr int kStatsThreads = 256;
+
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__device__ __forceinline__ double from_ordered_bits(unsigned long long o) {
+  const unsigned long long b = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+  return __longlong_as_double((long long)b);
+}
+
+struct StatAcc {
+  double mn[3], sm[3], mx[3];
+};
+
+__device__ __forceinline__ void stat_add(StatAcc &s, int k, double v) {
+  s.mn[k] = fmin(s.mn[k], v);
+  s.mx[k] = fmax(s.mx[k], v);
+  s.sm[k] += v;
+}
+
+template <int Q, int S, bool FORCE>
+__global__ void __launch_bounds__(kStatsThreads) k_stats(const StepArgs a,
+                                                         unsigned long long *out) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  using R = typename St::R;
+  using V = VSet<Q>;
+  __shared__ StatAcc sh[kStatsThreads / 32];
+  StatAcc acc;
+  for (int k = 0; k < 3; ++k) {
+    acc.mn[k] = INFINITY;
+    acc.mx[k] = -INFINITY;
+    acc.sm[k] = 0.0;
+  }
+  const R *face_rho = static_cast<const R *>(a.face_rho_in);
+  unsigned bad = 0;
+  for (unsigned idx = blockIdx.x * kStatsThreads + threadIdx.x; idx < (unsigned)a.g.n;
+       idx += gridDim.x * kStatsThreads) {
+    int x, y, z;
+    const ChunkForce cf = chunk_force<FORCE>(a, idx);
+    a.dec(idx, x, y, z);
+    const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
+    R f[Q];
+    if (row_in)
+      pull_row_node<Q, S, true>(a.p, a.g, face_rho, idx, x, y, z, f);
+    else
+      pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, face_rho, f);
+    R rho, ux, uy, uz;
+    finish_node_m<Q, FORCE, St::kDev>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1,
+                                      cf, bad, rho, ux, uy, uz);
+    R fmn = R(INFINITY), fmx = -R(INFINITY);
+    double fsum = 0.0;
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      const R v = St::kDev ? f[i] + V::template wr<R>(i) : f[i];
+      fsum += (double)v;
+      fmn = fmin(fmn, v);
+      fmx = fmax(fmx, v);
+    });
+    acc.mn[0] = fmin(acc.mn[0], (double)fmn);
+    acc.mx[0] = fmax(acc.mx[0], (double)fmx);
+    acc.sm[0] += fsum;
+    stat_add(acc, 1, (double)ux);
+    stat_add(acc, 1, (double)uy);
+    stat_add(acc, 1, (double)uz);
+    stat_add(acc, 2, (double)rho);
+  }
+  report_bad(a.status, bad);
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      acc.mn[k] = fmin(acc.mn[k], __shfl_xor_sync(0xffffffffu, acc.mn[k], o));
+      acc.mx[k] = fmax(acc.mx[k], __shfl_xor_sync(0xffffffffu, acc.mx[k], o));
+      acc.sm[k] += __shfl_xor_sync(0xffffffffu, acc.sm[k], o);
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    StatAcc t = sh[0];
+    for (int w = 1; w < kStatsThreads / 32; ++w)
+      for (int k = 0; k < 3; ++k) {
+        t.mn[k] = fmin(t.mn[k], sh[w].mn[k]);
+        t.mx[k] = fmax(t.mx[k], sh[w].mx[k]);
+        t.sm[k] += sh[w].sm[k];
+      }
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(out + 3 * k, ordered_bits(t.mn[k]));
+      atomicAdd(reinterpret_cast<double *>(out + 3 * k + 1), t.sm[k]);
+      atomicMax(out + 3 * k + 2, ordered_bits(t.mx[k]));
+    }
+  }
+}
+
+// slots of the 9 statistics: min / max keys of +inf / -inf, sums 0
+__global__ void k_stats_init(unsigned long long *out) {
+  const int k = threadIdx.x;
+  if (k >= 9) return;
+  const int c = k % 3;
+  out[k] = c == 0 ? ordered_bits(INFINITY)
+                  : c == 2 ? ordered_bits(-INFINITY) : (unsigned long long)__double_as_longlong(0.0);
+}
+
+// in place: keys -> min / max, sums -> means over n*q, 3n and n values
+__global__ void k_stats_finish(unsigned long long *out, double n, double q) {
+  const int k = threadIdx.x;
+  if (k >= 9) return;
+  const int c = k % 3;
+  double v;
+  if (c == 1) {
+    const double count = k == 1 ? n * q : k == 4 ? 3.0 * n : n;
+    v = __longlong_as_double((long long)out[k]) / count;
+  } else {
+    v = from_ordered_bits(out[k]);
+  }
+  reinterpret_cast<double *>(out)[k] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -900,6 +1044,25 @@ struct StepLauncher {
     return LBM_OK;
   }
 };
+
+// Step statistics of velocity set Q and storage S: init, k_stats (eight
+// blocks per SM at most; the kernel streams the populations once), finish.
+template <int Q, int S>
+int run_stats_qs(const StepArgs &a, bool force, unsigned long long *out, cudaStream_t s) {
+  DeviceInfo d;
+  int sms = 148;
+  if (device_info(d)) sms = d.sms;
+  const unsigned blocks = (unsigned)std::min<long long>(blocks_for(a.g.n, kStatsThreads),
+                                                        (long long)sms * 8);
+  k_stats_init<<<1, 32, 0, s>>>(out);
+  if (force)
+    k_stats<Q, S, true><<<blocks, kStatsThreads, 0, s>>>(a, out);
+  else
+    k_stats<Q, S, false><<<blocks, kStatsThreads, 0, s>>>(a, out);
+  k_stats_finish<<<1, 32, 0, s>>>(out, (double)a.g.n, (double)Q);
+  LBM_LAUNCH_CHECK("lbm_flow_stats");
+  return LBM_OK;
+}
 
 // Multi-lattice launch for velocity set Q and storage S: nodes per thread 1
 // (256 threads), 2 or 4 (128 threads).

@@ -10,4 +10,6 @@ namespace lbm {
 template int run_step_qs<LBM_Q, LBM_S>(const StepArgs &, bool, int, int, cudaStream_t);
 template int run_step_batch_qs<LBM_Q, LBM_S>(const StepArgs *, const unsigned *, int, unsigned,
                                              bool, int, cudaStream_t);
+template int run_stats_qs<LBM_Q, LBM_S>(const StepArgs &, bool, unsigned long long *,
+                                        cudaStream_t);
 }  // namespace lbm

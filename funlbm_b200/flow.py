@@ -161,10 +161,6 @@ class Flow:
                                               self.config.Re, self.config.mu)
 
 
-def _tf(t):
-    return float(t.detach().float().cpu())
-
-
 class FlowD3(Flow):
     """3-D flow on liblbm_b200.so (flow/d3/base.py:57-323)."""
 
@@ -493,21 +489,43 @@ class FlowD3(Flow):
         return self._x
 
     # -- reporting (flow/base.py:183-206) ---------------------------------------
+    def step_stats(self):
+        """min, mean, max of f, u and rho at the end of the last step as a
+        float64 device tensor of 9 values, without a host synchronisation.
+        In the fused form one reduction kernel streams the populations once
+        (lbm_flow_stats); otherwise the reference tensors are reduced."""
+        if self._mode == "fused" and not self._obs_valid and self._last_force is not None:
+            return self._lat.stats(self._last_force[0])
+        vals = []
+        for t in (self.f, self.u, self.rou):
+            vals += [t.min(), t.double().mean(), t.max()]
+        return torch.stack([v.double() for v in vals])
+
     def to_json(self):
-        out = {}
-        for key, t in (("f", self.f), ("u", self.u), ("rho", self.rou)):
-            out[key] = [_tf(t.min()), _tf(t.mean()), _tf(t.max())]
-        return out
+        v = self.step_stats().tolist()
+        return {"f": v[0:3], "u": v[3:6], "rho": v[6:9]}
 
     def dump_checkpoint(self, group=None, *args, **kwargs):
+        """flow/base.py:208-211: ``f``; also ``FOL`` (not in the reference's
+        file), the force the end-of-step moments include, so that a loaded
+        state continues exactly as the saved run would have."""
         if group is not None:
             group.create_dataset("f", data=self.f.cpu().numpy(), compression="gzip",
                                  compression_opts=9)
+            group.create_dataset("FOL", data=self.FOL.cpu().numpy(), compression="gzip",
+                                 compression_opts=9)
 
     def load_checkpoint(self, group=None, *args, **kwargs):
+        """flow/base.py:213-216 (with the reference's tensor-construction
+        TypeError fixed): f, then the moments; FOL when the file has it."""
         if group is None:
             return
+        if getattr(self, "_fp64", False):
+            self._fp64_only_fused("load_checkpoint")
         self.f = torch.tensor(np.asarray(group.get("f")[:]), dtype=torch.float32, device=self.device)
+        fol = group.get("FOL")
+        if fol is not None:
+            self.FOL = torch.tensor(np.asarray(fol[:]), dtype=torch.float32, device=self.device)
         self.update_u_rou()
 
 

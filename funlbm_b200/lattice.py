@@ -170,6 +170,17 @@ class Lattice:
              None if force is None else ctypes_ref(force), ptr(self.face_rho[prev]), None,
              ctypes_ref(obs), None, self.stream())
 
+    def stats(self, force, out=None):
+        """min, mean, max of f, u, rho at the end of the last step (9 float64
+        values on the device), from the buffer the last step streamed from."""
+        prev = self.cur ^ 1
+        if out is None:
+            out = torch.empty(9, dtype=torch.float64, device=self.device)
+        call("lbm_flow_stats", ctypes_ref(self.desc), ptr(self.buf[prev]),
+             None if force is None else ctypes_ref(force), ptr(self.face_rho[prev]), ptr(out),
+             ptr(self.status), self.stream())
+        return out
+
     def set_launch_shape(self, nodes=0, threads=0):
         """Launch shape of the fused step (see funlbm_b200.tune)."""
         for d in (self.desc,):

@@ -18,7 +18,11 @@ reference, which logs every step), ``graph_steps`` (``run`` replays the
 fused steps between logging / checkpoint steps from captured CUDA graphs of
 up to this many steps; default 32, 0 = never), ``ibm.mode`` (``reference`` = the
 reference's last-writer-wins spreading, ``accumulate`` = summed spreading),
-``flow.precision.storage``, ``flow.body_force``, ``flow.init_field``.
+``flow.precision.storage``, ``flow.body_force``, ``flow.init_field``,
+``log.db`` (a SQLite file for the per-step records the reference keeps in
+its key-value store; default none).  Logging at the cadence runs off the
+step loop (funlbm_b200.steplog); ``save_bak`` writes the reference's VTK /
+Tecplot files headlessly (funlbm_b200.output).
 """
 from __future__ import annotations
 
@@ -36,6 +40,7 @@ from .config import BaseConfig, FileConfig, deep_get
 from .flow import FlowConfig, FlowD3, create_flow
 from .lattice import ctypes_ref, make_force
 from .particle import ParticleConfig, ParticleSwarm, create_particle_swarm
+from .steplog import StepLogWriter, StepStore, particle_log_tensor
 
 logger = logging.getLogger("funlbm_b200")
 
@@ -57,6 +62,7 @@ class Config(BaseConfig):
         self.log_per_steps = 1
         self.ibm_mode = "reference"
         self.graph_steps = 32
+        self.log_db = None
 
     def _from_json(self, config_json: dict, *args, **kwargs) -> "Config":
         self.dt = deep_get(config_json, "dt") or self.dt
@@ -76,6 +82,7 @@ class Config(BaseConfig):
         self.log_per_steps = int(deep_get(config_json, "log_per_steps") or self.log_per_steps)
         gs = deep_get(config_json, "graph_steps")
         self.graph_steps = self.graph_steps if gs is None else int(gs)
+        self.log_db = deep_get(config_json, "log.db") or self.log_db
         self.ibm_mode = deep_get(config_json, "ibm.mode") or self.ibm_mode
         if self.ibm_mode not in ("reference", "accumulate"):
             raise ValueError("ibm.mode must be 'reference' or 'accumulate'")
@@ -120,6 +127,7 @@ class LBMBase:
         self.init()
         total_steps = min(max_steps, self.config.max_step)
         self._run_loop(total_steps)
+        self.flush_log()
 
     def run_steps(self, count: int) -> None:
         """Advance ``count`` steps from ``self.step`` the way ``run`` does
@@ -214,15 +222,27 @@ class LBMBase:
         if self.step % max(1, self.config.log_per_steps):
             return
         self.check_status()
-        if not logger.isEnabledFor(logging.INFO):
+        if not logger.isEnabledFor(logging.INFO) and not self.config.log_db:
             return
-        fl = self.flow
-        info = ["step=%6d" % self.step]
-        for key, t in (("f", fl.f), ("u", fl.u), ("rho", fl.rou)):
-            info.append(key + "=" + ",".join("%.6f" % float(v) for v in (t.min(), t.mean(), t.max())))
-        for particle in self.particle_swarm.particles:
-            info.append(particle.to_str(self.step))
-        logger.info("\t".join(info))
+        # the line (and the SQLite record) from device reductions, copied
+        # asynchronously and written by a background thread
+        parts = self.particle_swarm.particles
+        pvals = torch.cat([particle_log_tensor(p) for p in parts]) if parts else None
+        self._step_log().submit(self.step, self.flow.step_stats(), pvals,
+                                [float(p.mass) for p in parts])
+
+    def _step_log(self):
+        w = self.__dict__.get("_log_writer")
+        if w is None:
+            store = StepStore(self.config.log_db) if self.config.log_db else None
+            w = self._log_writer = StepLogWriter(logger, store)
+        return w
+
+    def flush_log(self):
+        """Wait until every logged step has been written."""
+        w = self.__dict__.get("_log_writer")
+        if w is not None:
+            w.flush()
 
     def check_status(self):
         word = self.flow.read_status()
@@ -499,6 +519,28 @@ class LBMD3(LBMBase):
         g = self.body_force
         if g != (0.0, 0.0, 0.0):
             fl._FOL += torch.tensor(g, device=self.device, dtype=torch.float32)
+
+    # -- field output (lbm/lbm3d.py:169-244) -------------------------------------
+    def save_bak(self, step=10, *args, **kwargs):
+        """The reference's VTK / Tecplot output every ``file.per_steps`` steps:
+        flow u, rho, p on the nodes and each particle's markers, written by a
+        background thread from pinned copies (funlbm_b200.output)."""
+        if step % self.config.file_config.per_steps > 0:
+            return
+        from .output import AsyncWriter, snapshot
+
+        w = self.__dict__.get("_out_writer")
+        if w is None:
+            w = self._out_writer = AsyncWriter()
+        snap, ev = snapshot(self)
+        w.submit(snap, ev, step, self.config.file_config.vtk_path,
+                 self.config.file_config.tecplot_path)
+
+    def flush_output(self):
+        """Wait until every queued save_bak snapshot is on disk."""
+        w = self.__dict__.get("_out_writer")
+        if w is not None:
+            w.flush()
 
     def _ensure_status(self):
         if self._status_ibm is None:

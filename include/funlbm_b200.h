@@ -145,6 +145,16 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
                   const float *face_rho_in, float *face_rho_out, const lbm_observe *obs,
                   uint32_t *status, void *stream);
 
+/* Statistics of the state at the end of the step that streams from `fa`
+ * (the reference's f after cul_equ2, rou / u after the second update_u_rou)
+ * without materialising it: FlowD3.to_json (flow/base.py:183-206) as
+ * LBMBase._log_step_info logs it (lbm/base.py:105-144).  Reads the
+ * populations once and writes `out`, a device buffer of 9 doubles (8-byte
+ * aligned): min, mean, max of f (over all nodes and directions), of u (all
+ * components) and of rho.  Arguments as lbm_flow_step with fb = NULL. */
+int lbm_flow_stats(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                   const float *face_rho_in, double *out, uint32_t *status, void *stream);
+
 /* ---- many lattices per launch (serving) ---------------------------------
  * One fused step (as lbm_flow_step) for up to thousands of independent
  * lattices of one velocity set and storage in a single launch -- the form
