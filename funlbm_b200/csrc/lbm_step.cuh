@@ -305,7 +305,10 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const StepArgs a,
   }
 }
 
-// slots of the 9 statistics: min / max keys of +inf / -inf, sums 0
+// slots of the 9 statistics: min / max keys of +inf / -inf, sums 0 (a
+// template, instantiated beside each k_stats, so that every translation unit
+// that includes this header may carry it)
+template <int Q>
 __global__ void k_stats_init(unsigned long long *out) {
   const int k = threadIdx.x;
   if (k >= 9) return;
@@ -315,13 +318,14 @@ __global__ void k_stats_init(unsigned long long *out) {
 }
 
 // in place: keys -> min / max, sums -> means over n*q, 3n and n values
-__global__ void k_stats_finish(unsigned long long *out, double n, double q) {
+template <int Q>
+__global__ void k_stats_finish(unsigned long long *out, double n) {
   const int k = threadIdx.x;
   if (k >= 9) return;
   const int c = k % 3;
   double v;
   if (c == 1) {
-    const double count = k == 1 ? n * q : k == 4 ? 3.0 * n : n;
+    const double count = k == 1 ? n * Q : k == 4 ? 3.0 * n : n;
     v = __longlong_as_double((long long)out[k]) / count;
   } else {
     v = from_ordered_bits(out[k]);
@@ -1054,12 +1058,12 @@ int run_stats_qs(const StepArgs &a, bool force, unsigned long long *out, cudaStr
   if (device_info(d)) sms = d.sms;
   const unsigned blocks = (unsigned)std::min<long long>(blocks_for(a.g.n, kStatsThreads),
                                                         (long long)sms * 8);
-  k_stats_init<<<1, 32, 0, s>>>(out);
+  k_stats_init<Q><<<1, 32, 0, s>>>(out);
   if (force)
     k_stats<Q, S, true><<<blocks, kStatsThreads, 0, s>>>(a, out);
   else
     k_stats<Q, S, false><<<blocks, kStatsThreads, 0, s>>>(a, out);
-  k_stats_finish<<<1, 32, 0, s>>>(out, (double)a.g.n, (double)Q);
+  k_stats_finish<Q><<<1, 32, 0, s>>>(out, (double)a.g.n);
   LBM_LAUNCH_CHECK("lbm_flow_stats");
   return LBM_OK;
 }
