@@ -45,7 +45,7 @@ os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 Q = 19
 TAU_MU = 1.0 / 30.0
 U0 = 0.05
-BYTES_PER_LU = {"fp32": 2 * Q * 4, "fp16s": 2 * Q * 2, "bf16s": 2 * Q * 2}
+BYTES_PER_LU = {"fp32": 2 * Q * 4, "fp16s": 2 * Q * 2, "bf16s": 2 * Q * 2, "fp64": 2 * Q * 8}
 REF_DIR = os.path.join(ROOT, "baseline", "_ref")
 REF_STUBS = os.path.join(ROOT, "tests", "golden", "_stubs")
 FACE_NAMES = ("input", "output", "back", "forward", "bottom", "top")
@@ -65,6 +65,17 @@ def parse():
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16s", "bf16s"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp16s", action="store_true",
+                    help="skip the fp16s sub-object of the fp32 headline line")
+    ap.add_argument("--vs-fp64", action="store_true",
+                    help="with --case: run the case in fp64, fp32, fp16s and bf16s storage and "
+                         "report each one's error against the fp64 run")
+    ap.add_argument("--case-steps", type=int, default=None,
+                    help="steps of the --vs-fp64 runs (default: the case's stated horizon)")
+    ap.add_argument("--ke-errors", action="store_true",
+                    help="throughput sweep's accuracy: kinetic-energy decay of the periodic "
+                         "Taylor-Green vortex, D3Q13/15/19/27 x sizes x fp32/fp16s vs fp64")
+    ap.add_argument("--ke-sizes", type=int, nargs="+", default=[128, 256, 512])
     ap.add_argument("--cpu-size", type=int, default=64)
     ap.add_argument("--serve", action="store_true",
                     help="run the served-stream benchmark and print its own line")
@@ -716,6 +727,127 @@ def run_case_sphere(args):
             "status": int(lbm.check_status())}
 
 
+def _fields64(lbm):
+    """End-of-step rho, u and every particle's cx, cu as float64 host arrays."""
+    ps = lbm.particle_swarm.particles
+    return {"rho": lbm.flow.rou.double().cpu().numpy(), "u": lbm.flow.u.double().cpu().numpy(),
+            "cx": np.stack([p.cx.double().cpu().numpy() for p in ps]) if ps else None,
+            "cu": np.stack([p.cu.double().cpu().numpy() for p in ps]) if ps else None}
+
+
+def run_case_precision(args):
+    """The case (--case) at its stated horizon in FP64 storage and then in
+    fp32, fp16s and bf16s storage from the same seeded configuration; each
+    one's error against the FP64 run: rho relative, u normalised by max|u|,
+    particle position and velocity in lattice units (max over particles and
+    over the checkpoints every `every` steps)."""
+    import torch
+
+    from funlbm_b200.lbm import LBMD3, Config
+
+    horizon = {"ellipsoids": 3000, "sphere": 5000}[args.case]
+    steps = args.case_steps or horizon
+    every = max(1, steps // 10)
+    make = ellipsoids_config if args.case == "ellipsoids" else sphere_config
+
+    def one(storage):
+        lbm = LBMD3(config=Config().from_json(make(storage)))
+        lbm.init()
+        traj = []
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        done = 0
+        while done < steps:
+            k = min(every, steps - done)
+            lbm.run_steps(k)
+            done += k
+            ps = lbm.particle_swarm.particles
+            traj.append((np.stack([p.cx.double().cpu().numpy() for p in ps]),
+                         np.stack([p.cu.double().cpu().numpy() for p in ps])))
+        b.record()
+        torch.cuda.synchronize()
+        out = _fields64(lbm)
+        out["traj"] = traj
+        out["ms_per_step"] = a.elapsed_time(b) / steps
+        out["status"] = int(lbm.check_status())
+        out["markers"] = int(lbm.particle_swarm.struct().n_markers)
+        out["nodes"] = lbm.flow.n
+        del lbm
+        torch.cuda.empty_cache()
+        return out
+
+    ref = one("fp64")
+    res = {}
+    for storage in ("fp32", "fp16s", "bf16s"):
+        got = one(storage)
+        umax = np.abs(ref["u"]).max()
+        ex = max(np.abs(g[0] - r[0]).max() for g, r in zip(got["traj"], ref["traj"]))
+        eu = max(np.abs(g[1] - r[1]).max() for g, r in zip(got["traj"], ref["traj"]))
+        res[storage] = {
+            "rho_rel_err": float(np.abs(got["rho"] - ref["rho"]).max() / np.abs(ref["rho"]).max()),
+            "u_err_of_umax": float(np.abs(got["u"] - ref["u"]).max() / umax),
+            "cx_err_lu": float(ex), "cu_err_lu": float(eu),
+            "ms_per_step": got["ms_per_step"], "status": got["status"]}
+    return {"metric": "error vs the FP64 run of the same seed (%s, %d steps)" % (args.case, steps),
+            "case": args.case, "steps": steps, "checkpoints_every": every,
+            "nodes": ref["nodes"], "markers": ref["markers"],
+            "fp64": {"ms_per_step": ref["ms_per_step"], "status": ref["status"],
+                     "max_abs_u": float(np.abs(ref["u"]).max())},
+            "errors": res}
+
+
+def run_ke_errors(args, steps=200, every=20):
+    """Accuracy of the throughput sweep: the periodic Taylor-Green vortex
+    (u0 = 0.05, tau 0.6) for each velocity set and size, stored in fp32 and
+    fp16s, against FP64 storage of the same case: the largest relative
+    difference of the kinetic energy 1/2 sum rho |u|^2 over the samples every
+    `every` steps, and the final rho / u errors."""
+    import torch
+
+    from funlbm_b200.lbm import LBMD3, Config
+
+    def one(q, n, storage):
+        faces = ("input", "output", "back", "forward", "bottom", "top")
+        cfg = {"device": "cuda", "log_per_steps": 10 ** 9, "file": {"per_steps": 10 ** 9},
+               "flow": {"size": [n - 1] * 3, "param_type": "D3Q%d" % q,
+                        "param": {"mu": TAU_MU}, "precision": {"storage": storage},
+                        "init_field": {"type": "taylor_green", "u0": U0},
+                        "boundary": {k: {"code": "PERIODICAL"} for k in faces}}}
+        lbm = LBMD3(config=Config().from_json(cfg))
+        lbm.init()
+        ke = []
+        for _ in range(steps // every):
+            lbm.run_steps(every)
+            u = lbm.flow.u.double()
+            rho = lbm.flow.rou.double()
+            ke.append(float(0.5 * (rho * (u * u).sum(-1, keepdim=True)).sum()))
+        out = (np.array(ke), lbm.flow.rou.double().cpu().numpy(), lbm.flow.u.double().cpu().numpy())
+        del lbm, u, rho
+        torch.cuda.empty_cache()
+        return out
+
+    rows = []
+    for n in args.ke_sizes:
+        for q in (13, 15, 19, 27):
+            try:
+                ref = one(q, n, "fp64")
+                for storage in ("fp32", "fp16s"):
+                    ke, rho, u = one(q, n, storage)
+                    rows.append({"q": q, "n": n, "storage": storage, "steps": steps,
+                                 "ke_rel_err": float(np.abs(ke - ref[0]).max() / ref[0].min()),
+                                 "ke_decay": float(1 - ref[0][-1] / ref[0][0]),
+                                 "rho_rel_err": float(np.abs(rho - ref[1]).max()),
+                                 "u_err_of_umax": float(np.abs(u - ref[2]).max()
+                                                        / np.abs(ref[2]).max())})
+                del ref
+            except torch.cuda.OutOfMemoryError:
+                torch.cuda.empty_cache()
+                rows.append({"q": q, "n": n, "skipped": "device memory"})
+    return {"metric": "kinetic-energy decay error vs FP64 (periodic Taylor-Green, tau 0.6)",
+            "rows": rows}
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -805,9 +937,14 @@ def main():
 
     build.build()
     world, rank, local = dist_setup(args)
+    if args.ke_errors:
+        if rank == 0:
+            print(json.dumps(run_ke_errors(args)), flush=True)
+        return 0
     if args.case is not None:
         if rank == 0:
-            print(json.dumps(run_case_sphere(args)), flush=True)
+            res = run_case_precision(args) if args.vs_fp64 else run_case_sphere(args)
+            print(json.dumps(res), flush=True)
         return 0
     if args.serve:
         if rank == 0:
@@ -824,6 +961,23 @@ def main():
     peak, peak_kind = measured_peak()
     bytes_per_launch = BYTES_PER_LU[args.storage] * nodes
     achieved = bytes_per_launch / (ms_per_step / 1e3) / 1e9
+    fp16s = None
+    if args.storage == "fp32" and not args.no_fp16s:
+        # the same workload in FP16 shifted storage (half the bytes per update)
+        a16 = argparse.Namespace(**vars(args))
+        a16.storage = "fp16s"
+        ms16, clocks16, status16, launch16 = run_device(a16, world, rank, local)
+        step16 = ms16 / args.steps
+        b16 = BYTES_PER_LU["fp16s"] * nodes
+        ach16 = b16 / (step16 / 1e3) / 1e9
+        v16 = world * nodes * args.steps / (ms16 / 1e3) / 1e6
+        fp16s = {"value": v16, "unit": "MLUPS", "ms_per_step": step16, "vs_fp32": v16 / value,
+                 "launch_shape": {"nodes_per_thread": launch16[0],
+                                  "threads_per_block": launch16[1]},
+                 "roofline": {"bound": "hbm", "achieved": ach16, "peak": peak, "unit": "GB/s",
+                              "frac": ach16 / peak, "peak_kind": peak_kind,
+                              "algorithmic_bytes_per_launch": b16},
+                 "clocks": clocks16, "device_status": status16}
     e2e = None
     if not args.no_e2e:
         sec, h2d, d2h = run_e2e(args, world, local)
@@ -860,6 +1014,8 @@ def main():
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks,
         "device_status": status,
     }
+    if fp16s is not None:
+        line["fp16s"] = fp16s
     print(json.dumps(line), flush=True)
     return 0
 

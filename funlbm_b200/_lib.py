@@ -46,6 +46,7 @@ class LbmLattice(ctypes.Structure):
         ("neq_profile", ctypes.c_void_p),
         ("step_nodes", ctypes.c_int32),
         ("step_threads", ctypes.c_int32),
+        ("pz", ctypes.c_int32),
     ]
 
 

@@ -59,6 +59,12 @@ int check_lattice(const lbm_lattice *lat) {
     set_error("relaxation time tau=%g must exceed 0.5", (double)lat->tau);
     return LBM_ERR_INVALID;
   }
+  if (lat->pz != 0 && (lat->pz < lat->nz ||
+                       (long long)lat->nx * lat->ny * lat->pz >= (1ll << 31))) {
+    set_error("row pitch %d must be 0 or at least nz = %d (and the pitched lattice under "
+              "2^31 elements per direction)", lat->pz, lat->nz);
+    return LBM_ERR_INVALID;
+  }
   if (lat->storage < LBM_STORAGE_FP32 || lat->storage > LBM_STORAGE_FP64) {
     set_error("unknown population storage %d", lat->storage);
     return LBM_ERR_INVALID;
@@ -91,6 +97,9 @@ Geom make_geom(const lbm_lattice *lat) {
   g.nz = lat->nz;
   g.nyz = (long long)lat->ny * lat->nz;
   g.n = g.nyz * lat->nx;
+  g.pz = lat->pz > 0 ? lat->pz : lat->nz;
+  g.nyzp = (long long)lat->ny * g.pz;
+  g.np = g.nyzp * lat->nx;
   for (int i = 0; i < LBM_NFACES; ++i) {
     g.face[i] = lat->face[i];
     for (int k = 0; k < 3; ++k) g.uw[i][k] = lat->face_uw[i][k];
@@ -132,8 +141,8 @@ static void fill_planes_q(const Geom &g, const void *fa, void *fb, int elem, Ste
   const uintptr_t a = (uintptr_t)fa, b = (uintptr_t)fb;
   auto at = [&](uintptr_t base, long long e) { return base + (uintptr_t)(e * elem); };
   for (int i = 0; i < Q; ++i) {
-    const long long plane = (long long)i * g.n, rplane = (long long)V::rev(i) * g.n;
-    p.src[i] = (const void *)at(a, plane - (long long)V::ex(i) * g.nyz - (long long)V::ey(i) * g.nz);
+    const long long plane = (long long)i * g.np, rplane = (long long)V::rev(i) * g.np;
+    p.src[i] = (const void *)at(a, plane - (long long)V::ex(i) * g.nyzp - (long long)V::ey(i) * g.pz);
     p.zlo[i] = nullptr;
     p.zhi[i] = nullptr;
     if (V::ez(i) > 0)

@@ -50,8 +50,9 @@ __global__ void __launch_bounds__(kThreads)
   collide<Q>(f, g, rho, ux, uy, uz);
   if (face && face_rho_ != nullptr) write_face_rho<Q>(g, static_cast<R *>(face_rho_), x, y, z, rho);
   typename St::T *fa = static_cast<typename St::T *>(fa_);
+  const long long pidx = ((long long)x * g.ny + y) * g.pz + z;
 #pragma unroll
-  for (int i = 0; i < Q; ++i) St::store(fa + (long long)i * g.n + idx, f[i], V::template wr<R>(i));
+  for (int i = 0; i < Q; ++i) St::store(fa + (long long)i * g.np + pidx, f[i], V::template wr<R>(i));
 }
 
 // ---------------------------------------------------------------------------
@@ -306,6 +307,7 @@ static int build_step_args(const lbm_lattice *lat, const void *fa, void *fb, con
   memset(&a, 0, sizeof(a));
   a.g = make_geom(lat);
   a.dec = make_decomp(a.g);
+  a.pdec = NodeDecomp{make_fastdiv((unsigned)a.g.pz), make_fastdiv((unsigned)a.g.ny)};
   a.fa = fa;
   a.fb = fb;
   use_force = false;
@@ -367,9 +369,9 @@ int lbm_flow_step(const lbm_lattice *lat, const void *fa, void *fb, const lbm_fo
   if (rc) return rc;
   const int bits = storage_bits(lat->storage);
   if (lat->step_nodes != 0 && lat->step_nodes != LBM_STEP_ROWS &&
-      !step_shape_legal(lat->step_nodes, lat->nz, bits)) {
-    set_error("lbm_flow_step: %d nodes per thread does not fit rows of %d nodes (%d-bit storage)",
-              lat->step_nodes, lat->nz, bits);
+      !step_shape_legal(lat->step_nodes, a.g.pz, bits)) {
+    set_error("lbm_flow_step: %d nodes per thread does not fit rows of pitch %d (%d-bit storage)",
+              lat->step_nodes, a.g.pz, bits);
     return LBM_ERR_INVALID;
   }
   if (lat->step_threads != 0 && lat->step_threads != 128 && lat->step_threads != 256) {
@@ -420,13 +422,13 @@ int lbm_batch_pack(const lbm_lattice *lat, const void *fa, void *fb, const lbm_f
                            use_force, "lbm_batch_pack");
   if (rc) return rc;
   const int bits = storage_bits(lat->storage);
-  if (nodes != 1 && !((nodes == 2 || nodes == 4) && step_shape_ok(nodes, lat->nz, bits))) {
+  if (nodes != 1 && !((nodes == 2 || nodes == 4) && step_shape_ok(nodes, a.g.pz, bits))) {
     set_error("lbm_batch_pack: nodes per thread must be 1, or 2 / 4 for rows of a multiple of "
               "that many nodes (at least twice as many)");
     return LBM_ERR_INVALID;
   }
   const long long per_block = (nodes == 1 ? 256 : 128) * (long long)kBatchTiles;
-  const long long work = a.g.n / nodes;
+  const long long work = nodes == 1 ? a.g.n : a.g.np / nodes;
   *blocks = (uint32_t)((work + per_block - 1) / per_block);
   memcpy(entry, &a, sizeof(a));
   return LBM_OK;
@@ -458,6 +460,10 @@ int lbm_collide(const lbm_lattice *lat, float *f, const float *rho, const float 
                 void *stream) {
   int rc = check_lattice(lat);
   if (rc) return rc;
+  if (lat->pz != 0 && lat->pz != lat->nz) {
+    set_error("lbm_collide: the single-function calls take dense arrays (pz = 0 or nz)");
+    return LBM_ERR_INVALID;
+  }
   if (f == nullptr || rho == nullptr || u == nullptr) {
     set_error("lbm_collide: f, rho and u are required");
     return LBM_ERR_INVALID;
@@ -469,6 +475,10 @@ int lbm_stream(const lbm_lattice *lat, const float *f_in, float *f_out, const fl
                const float *feq, void *stream) {
   int rc = check_lattice(lat);
   if (rc) return rc;
+  if (lat->pz != 0 && lat->pz != lat->nz) {
+    set_error("lbm_stream: the single-function calls take dense arrays (pz = 0 or nz)");
+    return LBM_ERR_INVALID;
+  }
   if (f_in == nullptr || f_out == nullptr || f_in == f_out) {
     set_error("lbm_stream: needs distinct input and output buffers");
     return LBM_ERR_INVALID;
@@ -489,6 +499,10 @@ int lbm_moments(const lbm_lattice *lat, const float *f, const float *fol, float 
                 float *p, float *scratch, void *stream) {
   int rc = check_lattice(lat);
   if (rc) return rc;
+  if (lat->pz != 0 && lat->pz != lat->nz) {
+    set_error("lbm_moments: the single-function calls take dense arrays (pz = 0 or nz)");
+    return LBM_ERR_INVALID;
+  }
   if (f == nullptr || rho == nullptr || u == nullptr) {
     set_error("lbm_moments: f, rho and u are required");
     return LBM_ERR_INVALID;
@@ -516,6 +530,10 @@ int lbm_add_force(const lbm_lattice *lat, float *f, const float *u, const float 
                   void *stream) {
   int rc = check_lattice(lat);
   if (rc) return rc;
+  if (lat->pz != 0 && lat->pz != lat->nz) {
+    set_error("lbm_add_force: the single-function calls take dense arrays (pz = 0 or nz)");
+    return LBM_ERR_INVALID;
+  }
   if (f == nullptr || u == nullptr || fol == nullptr) {
     set_error("lbm_add_force: f, u and FOL are required");
     return LBM_ERR_INVALID;

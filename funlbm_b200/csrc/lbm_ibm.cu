@@ -150,8 +150,9 @@ __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
         const typename Storage<S>::T *fa = static_cast<const typename Storage<S>::T *>(a.fa);
         const R *face_rho = static_cast<const R *>(a.face_rho_in);
         R f[Q];
+        const unsigned pidx = (unsigned)(((long long)x * a.g.ny + y) * a.g.pz + z);
         if (x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1)
-          pull_row_node<Q, S, false>(a.planes, a.g, face_rho, (unsigned)idx, x, y, z, f);
+          pull_row_node<Q, S, false>(a.planes, a.g, face_rho, pidx, x, y, z, f);
         else
           pull_general<Q, S>(fa, a.g, x, y, z, face_rho, f);
         R fx = a.go[0], fy = a.go[1], fz = a.go[2];

@@ -256,6 +256,9 @@ struct Geom {
   int nx, ny, nz;
   long long n;      // nodes
   long long nyz;    // ny * nz
+  int pz;           // row pitch of the population buffers (>= nz)
+  long long np;     // population plane: nx * ny * pz elements
+  long long nyzp;   // ny * pz
   int face[LBM_NFACES];
   float uw[LBM_NFACES][3];
   long long plane_off[LBM_NFACES];  // offsets of the face-density planes
@@ -358,12 +361,12 @@ __device__ __forceinline__ typename Storage<S>::R pull_one(
       }
     }
   }
-  const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;
+  const long long src = ((long long)sx * g.ny + sy) * g.pz + sz;
   const R w_sd = sd == I ? V::template wr<R>(I) : V::template wr<R>(V::rev(I));
   if constexpr (WORK)
-    return Storage<S>::work(fa + (long long)sd * g.n + src) - corr;
+    return Storage<S>::work(fa + (long long)sd * g.np + src) - corr;
   else
-    return Storage<S>::load(fa + (long long)sd * g.n + src, w_sd) - corr;
+    return Storage<S>::load(fa + (long long)sd * g.np + src, w_sd) - corr;
 }
 
 template <int Q, int S, bool WORK, int I = 0>
@@ -396,7 +399,8 @@ constexpr int kMaxQ = 27;
 
 // Per-direction plane pointers of one step, computed on the host
 // (fill_step_planes), so that every population address in the kernels is
-// one 32 x 32 -> 64-bit multiply-add of the node index onto a parameter:
+// one 32 x 32 -> 64-bit multiply-add of the node's population index
+// (x ny + y) pz + z onto a parameter:
 //   src[i] + idx   row (x - ex, y - ey) of plane i of fa at the node's z: the
 //                  pull source of an interior row is src[i] + idx - ez;
 //   zlo[i] + idx   (ez > 0) source of a node at z = 0 under the bottom face
@@ -472,7 +476,7 @@ __device__ __forceinline__ float pull_rolled(const typename Storage<S>::T *__res
   sx = sx < 0 ? sx + g.nx : (sx >= g.nx ? sx - g.nx : sx);
   sy = sy < 0 ? sy + g.ny : (sy >= g.ny ? sy - g.ny : sy);
   sz = sz < 0 ? sz + g.nz : (sz >= g.nz ? sz - g.nz : sz);
-  const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;
+  const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;   // dense arrays only
   return Storage<S>::load(fa + (long long)i * g.n + src, V::w(i));
 }
 

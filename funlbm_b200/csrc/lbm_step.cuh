@@ -17,7 +17,8 @@ constexpr int kThreads = 256;
 // ---------------------------------------------------------------------------
 struct StepArgs {
   Geom g;
-  NodeDecomp dec;
+  NodeDecomp dec;    // dense node index -> (x, y, z)
+  NodeDecomp pdec;   // population index (x ny + y) pz + z -> (x, y, z)
   const void *fa;
   void *fb;
   float go[3], gn[3];
@@ -167,12 +168,13 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   int x, y, z;
   const ChunkForce cf = chunk_force<FORCE>(a, idx);
   a.dec(idx, x, y, z);
+  const unsigned pidx = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.pz + (unsigned)z;
   using R = typename St::R;
   const R *face_rho = static_cast<const R *>(a.face_rho_in);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   R f[Q];
   if (row_in)
-    pull_row_node<Q, S, true>(a.p, a.g, face_rho, idx, x, y, z, f);
+    pull_row_node<Q, S, true>(a.p, a.g, face_rho, pidx, x, y, z, f);
   else
     pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, face_rho, f);
   unsigned bad = 0;
@@ -182,7 +184,7 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   if (a.fb != nullptr) {
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      St::put(static_cast<T *>(a.p.dst[i]) + idx, f[i]);
+      St::put(static_cast<T *>(a.p.dst[i]) + pidx, f[i]);
     });
   }
 }
@@ -253,9 +255,10 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const StepArgs a,
     const ChunkForce cf = chunk_force<FORCE>(a, idx);
     a.dec(idx, x, y, z);
     const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
+    const unsigned pidx = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.pz + (unsigned)z;
     R f[Q];
     if (row_in)
-      pull_row_node<Q, S, true>(a.p, a.g, face_rho, idx, x, y, z, f);
+      pull_row_node<Q, S, true>(a.p, a.g, face_rho, pidx, x, y, z, f);
     else
       pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, face_rho, f);
     R rho, ux, uy, uz;
@@ -352,13 +355,14 @@ __host__ __device__ constexpr bool compact_face_rows() {
   return FORCE || (Q == 13 && Storage<S>::kBits == 16);
 }
 
-// Nodes of a row on an x / y face (under 1 % of a large lattice): one at a
-// time through the general face rules, in a loop that is not unrolled, so a
+// Nodes of a row on an x / y face (under 1 % of a large lattice), or the
+// last nodes of a row whose length is not a multiple of a thread's NZ: one at
+// a time through the general face rules, in a loop that is not unrolled, so a
 // vector kernel carries one copy of this code instead of NZ.  Same per-node
-// arithmetic.
+// arithmetic.  idx0 / pidx0: dense / population index of node (x, y, z0).
 template <int Q, int S, bool FORCE>
-__device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, int count, int x,
-                                               int y, int z0) {
+__device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, unsigned pidx0,
+                                               int count, int x, int y, int z0) {
   using St = Storage<S>;
   using T = typename St::T;
   using R = typename St::R;
@@ -369,13 +373,13 @@ __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0,
   for (int k = 0; k < count; ++k) {
     R f[Q];
     pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, face_rho, f);
-    // the nodes may lie in two chunks (pairs of odd-length rows)
-    finish_node<Q, FORCE, St::kDev>(a, f, idx0 + k, x, y, z0 + k, true,
+    // the nodes may lie in two chunks
+    finish_node<Q, FORCE, St::kDev>(a, f, idx0 + k, x, y, z0 + k, on_any_face(a.g, x, y, z0 + k),
                                     chunk_force<FORCE>(a, idx0 + k), bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        St::put(static_cast<T *>(a.p.dst[i]) + idx0 + k, f[i]);
+        St::put(static_cast<T *>(a.p.dst[i]) + pidx0 + k, f[i]);
       });
     }
   }
@@ -393,23 +397,27 @@ __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0,
 // its elements are loaded and stored one by one and its nodes may lie in two
 // different force chunks.
 template <int Q, int S, bool FORCE, int NZ, bool COMPACT, bool ALIGNED = true>
-__device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsigned idx0) {
+__device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsigned pidx0) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
   static_assert(St::kBits == 16 && NZ % 2 == 0, "pairs of 16-bit elements");
   static_assert(ALIGNED || NZ == 2, "unaligned pairs are single pairs");
   constexpr int kWords = NZ / 2;
-  if (idx0 >= (unsigned)a.g.n) return;
+  if (pidx0 >= (unsigned)a.g.np) return;
   int x, y, z0;
-  const ChunkForce cf = chunk_force<FORCE>(a, idx0);
-  const ChunkForce cf1 = ALIGNED ? cf : chunk_force<FORCE>(a, idx0 + 1);
-  a.dec(idx0, x, y, z0);
+  a.pdec(pidx0, x, y, z0);
+  if (z0 >= a.g.nz) return;                  // row padding
+  const unsigned idx0 = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.nz + (unsigned)z0;
+  if (z0 + NZ > a.g.nz) {                    // the last nodes of a row (pitched rows)
+    face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, a.g.nz - z0, x, y, z0);
+    return;
+  }
   constexpr bool kCompact = COMPACT;
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {
     if (!row_in) {
-      face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0);
+      face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, NZ, x, y, z0);
       return;
     }
     row_in = true;
@@ -421,15 +429,15 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       constexpr int ez = V::ez(i);
-      const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
+      const T *ps = static_cast<const T *>(a.p.src[i]) + pidx0;
       if constexpr (ALIGNED)
         raw[i] = ld_words<kWords>(ps);
       else
         raw[i].w[0] = (unsigned)bits16(St::raw(ps)) | ((unsigned)bits16(St::raw(ps + 1)) << 16);
       if constexpr (ez > 0)
-        extra[i] = St::raw(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx0 : ps - 1);
+        extra[i] = St::raw(bottom ? static_cast<const T *>(a.p.zlo[i]) + pidx0 : ps - 1);
       if constexpr (ez < 0)
-        extra[i] = St::raw(top ? static_cast<const T *>(a.p.zhi[i]) + (idx0 + NZ - 1) : ps + NZ);
+        extra[i] = St::raw(top ? static_cast<const T *>(a.p.zhi[i]) + (pidx0 + NZ - 1) : ps + NZ);
     });
   }
   unsigned bad = 0;
@@ -464,14 +472,17 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
       pull_general<Q, S, true>(fa, a.g, x, y, za, face_rho, f0);
       pull_general<Q, S, true>(fa, a.g, x, y, za + 1, face_rho, f1);
     }
+    // (a pair may straddle two force chunks: dense rows of any length)
     finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
-                                !row_in || za == 0 || za == a.g.nz - 1, cf, bad);
+                                !row_in || za == 0 || za == a.g.nz - 1,
+                                chunk_force<FORCE>(a, idx0 + 2 * pr), bad);
     finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
-                                !row_in || za + 1 == a.g.nz - 1, cf1, bad);
+                                !row_in || za + 1 == a.g.nz - 1,
+                                chunk_force<FORCE>(a, idx0 + 2 * pr + 1), bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        T *dst = static_cast<T *>(a.p.dst[i]) + idx0 + 2 * pr;
+        T *dst = static_cast<T *>(a.p.dst[i]) + pidx0 + 2 * pr;
         const unsigned word = put2<S>(f0[i], f1[i]);
         if constexpr (ALIGNED) {
           st_words(dst, Words<1>{{word}});
@@ -502,16 +513,21 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   }
   using R = typename St::R;
   constexpr int kWords = NZ * St::kBits / 32;
-  const unsigned idx0 = t * NZ;
-  if (idx0 >= (unsigned)a.g.n) return;
+  const unsigned pidx0 = t * NZ;
+  if (pidx0 >= (unsigned)a.g.np) return;
   int x, y, z0;
-  const ChunkForce cf = chunk_force<FORCE>(a, idx0);
-  a.dec(idx0, x, y, z0);
+  a.pdec(pidx0, x, y, z0);
+  if (z0 >= a.g.nz) return;                  // row padding
+  const unsigned idx0 = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.nz + (unsigned)z0;
+  if (z0 + NZ > a.g.nz) {                    // the last nodes of a row (pitched rows)
+    face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, a.g.nz - z0, x, y, z0);
+    return;
+  }
   constexpr bool kCompact = COMPACT;
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {
     if (!row_in) {
-      face_row_nodes<Q, S, FORCE>(a, idx0, NZ, x, y, z0);
+      face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, NZ, x, y, z0);
       return;
     }
     row_in = true;
@@ -523,7 +539,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       constexpr int ez = V::ez(i);
-      const T *ps = static_cast<const T *>(a.p.src[i]) + idx0;
+      const T *ps = static_cast<const T *>(a.p.src[i]) + pidx0;
       const Words<kWords> raw = ld_words<kWords>(ps);
       R v[NZ];
       if constexpr (St::kBits == 32) {
@@ -546,12 +562,12 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
       } else if constexpr (ez > 0) {
 #pragma unroll
         for (int k = 1; k < NZ; ++k) f[k][i] = v[k - 1];
-        f[0][i] = St::work(bottom ? static_cast<const T *>(a.p.zlo[i]) + idx0 : ps - 1);
+        f[0][i] = St::work(bottom ? static_cast<const T *>(a.p.zlo[i]) + pidx0 : ps - 1);
       } else {
 #pragma unroll
         for (int k = 0; k < NZ - 1; ++k) f[k][i] = v[k + 1];
         f[NZ - 1][i] =
-            St::work(top ? static_cast<const T *>(a.p.zhi[i]) + (idx0 + NZ - 1) : ps + NZ);
+            St::work(top ? static_cast<const T *>(a.p.zhi[i]) + (pidx0 + NZ - 1) : ps + NZ);
       }
     });
     if (bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
@@ -569,8 +585,10 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
 #pragma unroll
   for (int k = 0; k < NZ; ++k) {
     const int z = z0 + k;
+    // (a thread's nodes may straddle two force chunks: dense rows of any length)
     finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z,
-                                    !row_in || z == 0 || z == a.g.nz - 1, cf, bad);
+                                    !row_in || z == 0 || z == a.g.nz - 1,
+                                    chunk_force<FORCE>(a, idx0 + k), bad);
   }
   report_bad(a.status, bad);
   if (a.fb == nullptr) return;
@@ -590,7 +608,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
 #pragma unroll
       for (int k = 0; k < NZ / 2; ++k) raw.w[k] = put2<S>(f[2 * k][i], f[2 * k + 1][i]);
     }
-    st_words(static_cast<T *>(a.p.dst[i]) + idx0, raw);
+    st_words(static_cast<T *>(a.p.dst[i]) + pidx0, raw);
   });
 }
 
@@ -880,20 +898,21 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, cons
 }
 
 // Launch shape of the fused step: nodes per thread (1 = scalar kernel, or
-// NZ consecutive z-nodes moved as 4 / 8 / 16-byte vectors, nz a multiple of
-// NZ) and threads per block.
+// NZ consecutive z-nodes moved as 4 / 8 / 16-byte vectors, the row pitch pz a
+// multiple of NZ; the last nodes of a row that does not fill a thread's NZ
+// take the per-node path) and threads per block.
 // Shapes lbm_flow_step accepts: the above, plus 2 nodes per thread for
-// 16-bit rows of odd length (k_step_odd).
-inline bool step_shape_ok(int nodes, int nz, int bits);
-inline bool step_shape_legal(int nodes, int nz, int bits) {
-  return step_shape_ok(nodes, nz, bits) || (nodes == 2 && bits == 16 && nz % 2 == 1 && nz >= 3);
+// unpitched 16-bit rows of odd length (k_step_odd).
+inline bool step_shape_ok(int nodes, int pz, int bits);
+inline bool step_shape_legal(int nodes, int pz, int bits) {
+  return step_shape_ok(nodes, pz, bits) || (nodes == 2 && bits == 16 && pz % 2 == 1 && pz >= 3);
 }
 
-inline bool step_shape_ok(int nodes, int nz, int bits) {
+inline bool step_shape_ok(int nodes, int pz, int bits) {
   if (nodes == 1) return true;
   if (nodes != 2 && nodes != 4 && nodes != 8) return false;
   if (nodes * bits / 32 < 1 || nodes * bits / 32 > 4) return false;
-  return nz % nodes == 0 && nz >= 2 * nodes;
+  return pz % nodes == 0 && pz >= 2 * nodes;
 }
 
 // Shared-memory plan of the TMA-staged step for this device, or false when
@@ -920,6 +939,7 @@ inline bool tma_plan(const Geom &g, int q, int bits, const void *fa, TmaPlan &p,
                      size_t &smem, unsigned &grid) {
   const int elem = bits / 8;
   const long long row_bytes = (long long)g.nz * elem;
+  if (g.pz != g.nz) return false;   // whole rows are copied: no padding between them
   if (row_bytes % 16 != 0 || g.nz < 16 || ((uintptr_t)fa & 15u) != 0) return false;
   DeviceInfo d;
   if (!device_info(d)) return false;
@@ -976,7 +996,7 @@ struct StepLauncher {
 
   template <int NZ, int TB>
   static void go_vec(const StepArgs &a, bool force, cudaStream_t s) {
-    const unsigned nb = blocks_for(a.g.n / NZ, TB);
+    const unsigned nb = blocks_for(a.g.np / NZ, TB);
     if (force)
       k_step_vec<Q, S, true, NZ, TB><<<nb, TB, 0, s>>>(a);
     else
@@ -1007,7 +1027,7 @@ struct StepLauncher {
   static int go(const StepArgs &a, bool force, int nodes, int threads, cudaStream_t s) {
     constexpr int bits = Storage<S>::kBits;
     if (nodes == LBM_STEP_ROWS) return go_tma(a, force, s);
-    const bool odd_pairs = bits == 16 && a.g.nz % 2 == 1 && a.g.nz >= 3;
+    const bool odd_pairs = bits == 16 && a.g.pz % 2 == 1 && a.g.nz >= 3;
     if (nodes == 0) {
       // measured on B200 at 512^3: 2 nodes per thread with 128-thread blocks
       // is the fastest shape for every velocity set and storage, except
@@ -1017,7 +1037,7 @@ struct StepLauncher {
       const int want = (bits == 16 && Q == 19 && !force) ? 4 : 2;
       // (rows of odd length: one node per thread; the odd-row pair kernel
       // is only a tuner candidate -- measured no faster in general)
-      nodes = step_shape_ok(want, a.g.nz, bits) ? want : step_shape_ok(2, a.g.nz, bits) ? 2 : 1;
+      nodes = step_shape_ok(want, a.g.pz, bits) ? want : step_shape_ok(2, a.g.pz, bits) ? 2 : 1;
       threads = threads ? threads : 128;
     }
     if (nodes == 2 && odd_pairs) {

@@ -20,6 +20,19 @@ BC = {"PERIODICAL": 11000, "WALL": 1200, "WALL_WITH_SPEED": 1201, "NON_EQUILIBRI
 STORAGE_DTYPE = {"fp32": torch.float32, "fp16s": torch.float16, "bf16s": torch.bfloat16,
                  "fp64": torch.float64}
 BYTES = {"fp32": 4, "fp16s": 2, "bf16s": 2, "fp64": 8}
+# elements of the widest vector (16 bytes) the step moves per thread: the
+# population rows are pitched to a multiple of it
+VECTOR_ELEMS = {"fp32": 4, "fp16s": 8, "bf16s": 8, "fp64": 2}
+
+
+def row_pitch(nz, storage):
+    """Row pitch of the population buffers: nz rounded up to the widest vector,
+    so that rows of any length (the reference's size + 1 nodes are odd for
+    even sizes) run the vectorised step."""
+    w = VECTOR_ELEMS[storage]
+    return -(-int(nz) // w) * w
+
+
 # arithmetic type of a storage: what its fields, face densities, force fields
 # and observation buffers hold
 REAL_DTYPE = {"fp32": torch.float32, "fp16s": torch.float32, "bf16s": torch.float32,
@@ -59,12 +72,15 @@ class Lattice:
     """One lattice: descriptor, population buffers, face-density planes."""
 
     def __init__(self, q, shape, faces, tau, storage="fp32", face_uw=None, re_mu=0.0,
-                 device="cuda", allocate=True):
+                 device="cuda", allocate=True, pitch=True):
         if storage not in STORAGE_DTYPE:
             raise ValueError("unknown storage %r (fp32, fp16s, bf16s)" % (storage,))
         self.q = int(q)
         self.shape = tuple(int(s) for s in shape)
         self.n = self.shape[0] * self.shape[1] * self.shape[2]
+        # population rows pitched to the vector width (pitch=False: dense rows)
+        self.pz = row_pitch(self.shape[2], storage) if pitch else self.shape[2]
+        self.np = self.shape[0] * self.shape[1] * self.pz
         self.storage = storage
         self.device = torch.device(device)
         self.faces = [int(c) for c in faces]
@@ -77,7 +93,8 @@ class Lattice:
             prof = duct_profile(self.shape[1], self.shape[2])
             self._profile = torch.tensor(prof.reshape(-1), dtype=torch.float64, device=self.device)
         self.desc = self._make_desc(storage)
-        self.desc_fp32 = self._make_desc("fp32")
+        self.desc.pz = self.pz
+        self.desc_fp32 = self._make_desc("fp32")     # dense: the single-function calls
         call("lbm_lattice_check", ctypes_ref(self.desc))
         self.needs_face_rho = any(c in (BC["WALL_WITH_SPEED"], BC["NON_EQUILIBRIUM"]) for c in self.faces)
         self.fused = BC["NON_EQUILIBRIUM"] not in self.faces
@@ -106,7 +123,7 @@ class Lattice:
     # -- memory ------------------------------------------------------------
     @staticmethod
     def bytes_needed(q, shape, storage="fp32"):
-        n = int(shape[0]) * int(shape[1]) * int(shape[2])
+        n = int(shape[0]) * int(shape[1]) * row_pitch(shape[2], storage)
         planes = 2 * (shape[1] * shape[2] + shape[0] * shape[2] + shape[0] * shape[1])
         return 2 * q * n * BYTES[storage] + 2 * REAL_DTYPE[storage].itemsize * planes
 
@@ -114,7 +131,7 @@ class Lattice:
         dt = STORAGE_DTYPE[self.storage]
         for i in range(2):
             if self.buf[i] is None:
-                self.buf[i] = torch.empty(self.q * self.n, dtype=dt, device=self.device)
+                self.buf[i] = torch.empty(self.q * self.np, dtype=dt, device=self.device)
         if self.needs_face_rho and self.face_rho[0] is None:
             nplanes = _lib.load().lbm_face_plane_floats(ctypes_ref(self.desc))
             self.face_rho = [torch.zeros(nplanes, dtype=REAL_DTYPE[self.storage],
@@ -144,13 +161,16 @@ class Lattice:
              ptr(self.face_rho[self.cur]), self.stream())
 
     def load_post_collision_fp32(self, a):
-        """Adopt float32 SoA post-collision populations (storage conversion on device)."""
+        """Adopt float32 SoA post-collision populations (dense [q][x][y][z];
+        storage conversion and row pitch on the device)."""
+        X, Y, Z = self.shape
+        dst = self.buf[self.cur].view(self.q, X * Y, self.pz)[:, :, :Z]
+        src = a.reshape(self.q, X * Y, Z)
         if self.storage in ("fp32", "fp64"):
-            self.buf[self.cur].copy_(a.reshape(-1))
+            dst.copy_(src)
         else:
             w = weights_tensor(self.q, self.device)
-            dev = (a.view(self.q, -1) - w[:, None]).to(STORAGE_DTYPE[self.storage])
-            self.buf[self.cur].copy_(dev.reshape(-1))
+            dst.copy_((src - w[:, None, None]).to(STORAGE_DTYPE[self.storage]))
 
     def step(self, force=None, obs=None):
         nxt = self.cur ^ 1

@@ -359,7 +359,7 @@ class LBMServer:
     def _nodes_per_thread(lat):
         # two z-nodes per thread for float32 rows of even length; 16-bit
         # storage runs fastest with one node per thread
-        return 2 if lat.storage == "fp32" and lat.shape[2] % 2 == 0 and lat.shape[2] >= 4 else 1
+        return 2 if lat.storage == "fp32" and lat.pz % 2 == 0 and lat.pz >= 4 else 1
 
     def _pack_tables(self, plans):
         """Group the active lattices by (q, storage, nodes), pack their entries

@@ -25,26 +25,29 @@ _CACHE = {}
 PROXY_BYTES = 2 << 30          # populations of the proxy lattice (both buffers)
 
 
-def shape_ok(nodes, nz, bits):
+def shape_ok(nodes, pz, bits, nz=None):
+    """Whether the fused step accepts `nodes` per thread on rows of pitch pz
+    (nz: the row's node count when it differs from the pitch)."""
+    nz = pz if nz is None else nz
     if nodes == 1:
         return True
     if nodes == ROWS:
-        return bits != 64 and (nz * bits // 8) % 16 == 0 and nz >= 16
+        return bits != 64 and pz == nz and (nz * bits // 8) % 16 == 0 and nz >= 16
     if nodes * bits // 32 not in (1, 2, 4):
         return False
-    if nodes == 2 and bits == 16 and nz % 2 == 1 and nz >= 3:
-        return True                 # pairs within rows of odd length
-    return nz % nodes == 0 and nz >= 2 * nodes
+    if nodes == 2 and bits == 16 and pz % 2 == 1 and pz >= 3:
+        return True                 # pairs within unpitched rows of odd length
+    return pz % nodes == 0 and pz >= 2 * nodes
 
 
-def default_shape(q, storage, nz, forced=False):
+def default_shape(q, storage, pz, forced=False):
     """The launch shape lbm_flow_step uses when none is set (measured best at
     512^3): 2 nodes per thread with 128 threads, 4 for unforced D3Q19 in
     16-bit storage, one node per thread where rows allow no vector."""
     bits = STORAGE_BITS[storage]
     want = 4 if (bits == 16 and q == 19 and not forced) else 2
     for nodes in (want, 2):
-        if nz % nodes == 0 and nz >= 2 * nodes:
+        if pz % nodes == 0 and pz >= 2 * nodes:
             return (nodes, 128)
     return (1, 256)
 
@@ -68,7 +71,7 @@ def tune(lat, force=None, iters=6, warmup=2, verbose=False):
     from .lattice import BYTES, Lattice
 
     bits = STORAGE_BITS[lat.storage]
-    key = (lat.q, lat.storage, lat.shape[1], lat.shape[2], force is not None)
+    key = (lat.q, lat.storage, lat.shape[1], lat.shape[2], lat.pz, force is not None)
     if key in _CACHE:
         choice, timings = _CACHE[key]
         lat.set_launch_shape(*choice)
@@ -83,7 +86,7 @@ def tune(lat, force=None, iters=6, warmup=2, verbose=False):
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     for nodes, threads in CANDIDATES[bits]:
-        if not shape_ok(nodes, nz, bits):
+        if not shape_ok(nodes, proxy.pz, bits, nz):
             continue
         proxy.set_launch_shape(nodes, threads)
         for _ in range(warmup):
@@ -96,7 +99,7 @@ def tune(lat, force=None, iters=6, warmup=2, verbose=False):
         timings[(nodes, threads)] = start.elapsed_time(stop) / iters
     proxy.release()
     del proxy
-    choice = _pick(timings, default_shape(lat.q, lat.storage, nz, force is not None))
+    choice = _pick(timings, default_shape(lat.q, lat.storage, lat.pz, force is not None))
     if verbose:
         for k, v in sorted(timings.items(), key=lambda kv: kv[1]):
             print("tune q=%d %s %dx%dx%d (proxy nx=%d): nodes=%d threads=%d  %.4f ms"
@@ -110,13 +113,15 @@ _CLASS_CACHE = {}
 CLASS_PROXY_NODES = 96          # proxy lattice of a class: about 96^3 nodes
 
 
-def class_key_of(q, storage, nz, forced):
-    return (int(q), storage, nz % 2 == 0 and nz >= 4, nz % 4 == 0 and nz >= 8,
-            nz % 8 == 0 and nz >= 16, bool(forced))
+def class_key_of(q, storage, pz, forced):
+    """Class of a lattice for the tuner: velocity set, storage, the vector
+    widths its row pitch pz allows, forced or not."""
+    return (int(q), storage, pz % 2 == 0 and pz >= 4, pz % 4 == 0 and pz >= 8,
+            pz % 8 == 0 and pz >= 16, bool(forced))
 
 
 def class_key(lat, forced):
-    return class_key_of(lat.q, lat.storage, lat.shape[2], forced)
+    return class_key_of(lat.q, lat.storage, lat.pz, forced)
 
 
 def tune_class_of(q, storage, nz, forced, device="cuda", iters=6, warmup=2):
@@ -155,7 +160,7 @@ def tune_class_of(q, storage, nz, forced, device="cuda", iters=6, warmup=2):
     stop = torch.cuda.Event(enable_timing=True)
     timings = {}
     for nodes, threads in CANDIDATES[bits]:
-        if nodes == ROWS or not shape_ok(nodes, pnz, bits):
+        if nodes == ROWS or not shape_ok(nodes, proxy.pz, bits, pnz):
             continue
         proxy.set_launch_shape(nodes, threads)
         for _ in range(warmup):
@@ -166,15 +171,16 @@ def tune_class_of(q, storage, nz, forced, device="cuda", iters=6, warmup=2):
         stop.record()
         stop.synchronize()
         timings[(nodes, threads)] = start.elapsed_time(stop) / iters
+    ppz = proxy.pz
     proxy.release()
     del proxy
-    _CLASS_CACHE[key] = _pick(timings, default_shape(q, storage, pnz, forced))
+    _CLASS_CACHE[key] = _pick(timings, default_shape(q, storage, ppz, forced))
     return _CLASS_CACHE[key]
 
 
 def tune_class(lat, forced=False):
     """Set ``lat``'s launch shape to its class's tuned choice (tune_class_of)."""
-    choice = tune_class_of(lat.q, lat.storage, lat.shape[2], forced, device=lat.device)
+    choice = tune_class_of(lat.q, lat.storage, lat.pz, forced, device=lat.device)
     lat.set_launch_shape(*choice)
     return choice
 

@@ -90,6 +90,15 @@ typedef struct lbm_lattice {
                           /* storage / forcing)                                     */
   int32_t step_threads;   /* threads per block (128 or 256; 0 = 128 with the        */
                           /* default shape, else 256)                               */
+  int32_t pz;             /* row pitch of the population buffers in elements: a     */
+                          /* node (x, y, z) of direction i sits at                  */
+                          /* i*nx*ny*pz + (x*ny + y)*pz + z; pz >= nz, 0 = nz.      */
+                          /* Padding elements are never read as a source.  A pitch  */
+                          /* that is a multiple of the vector width lets rows of    */
+                          /* any length use the vectorised step.  Every other array */
+                          /* (fields, face planes, observation) stays dense.  The   */
+                          /* single-function calls (lbm_collide, lbm_stream,        */
+                          /* lbm_moments, lbm_add_force) take dense arrays only.    */
 } lbm_lattice;
 
 /* Forcing seen by one step: FOL = uniform + field.  `uniform` is a body force

@@ -480,3 +480,59 @@ def test_row_staged_wait_timeout_sets_status():
         lat.observe(force, f=f)
         results.append(to_np(f))
     assert np.array_equal(results[0], results[1])
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16s", "bf16s", "fp64"])
+@pytest.mark.parametrize("q", [15, 19, 27])
+def test_pitched_rows_agree_bitwise(q, storage):
+    """Population rows pitched to the vector width (rows of 13 and 33 nodes
+    stored in rows of 16 / 36 / 40 elements): every launch shape on the pitched
+    buffers -- vectors over full groups, the per-node path for the last nodes
+    of each row -- gives the bits of one node per thread on dense rows, with
+    WALL_WITH_SPEED z faces, walls and chunked force fields."""
+    from funlbm_b200.lattice import Lattice, make_force, tau_float32
+    from funlbm_b200.tune import CANDIDATES, STORAGE_BITS, shape_ok
+
+    rng = np.random.default_rng(50 + q)
+    bits = STORAGE_BITS[storage]
+    dt = torch.float64 if storage == "fp64" else torch.float32
+    for shape in ((9, 8, 13), (7, 6, 33)):
+        n = shape[0] * shape[1] * shape[2]
+        nch = (n + 31) // 32
+        kind = rng.integers(0, 4, nch)
+        ch_old = torch.tensor(((kind == 1) | (kind == 3)).astype(np.uint8), device="cuda")
+        ch_new = torch.tensor(((kind == 2) | (kind == 3)).astype(np.uint8), device="cuda")
+        node_kind = np.repeat(kind, 32)[:n]
+        f_old = 1e-4 * rng.standard_normal((n, 3))
+        f_new = 1e-4 * rng.standard_normal((n, 3))
+        f_old[~np.isin(node_kind, (1, 3))] = 0
+        f_new[~np.isin(node_kind, (2, 3))] = 0
+        F_old = torch.tensor(f_old.reshape(-1), device="cuda", dtype=dt)
+        F_new = torch.tensor(f_new.reshape(-1), device="cuda", dtype=dt)
+        force = make_force((0, 0, 0), (2e-6, 0, 0), F_old, F_new, ch_old, ch_new)
+        codes = [1200, 11000, 11000, 1200, 1201, 1201]
+        uw = (0.02 * rng.standard_normal((6, 3))).tolist()
+        f0 = smooth_f0(q, shape, 0.04, q + 7)
+        f0_soa = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda",
+                              dtype=dt)
+        results = {}
+        for pitch in (False, True):
+            for nodes, threads in CANDIDATES[bits]:
+                probe = Lattice(q, shape, codes, tau_float32(0.07), storage=storage, face_uw=uw,
+                                device="cuda", pitch=pitch, allocate=False)
+                if not shape_ok(nodes, probe.pz, bits, shape[2]) or (pitch and nodes == 1):
+                    continue
+                lat = Lattice(q, shape, codes, tau_float32(0.07), storage=storage, face_uw=uw,
+                              device="cuda", pitch=pitch)
+                lat.set_launch_shape(nodes, threads)
+                lat.init(f0_soa)
+                for _ in range(4):
+                    lat.step(force)
+                assert lat.read_status() == 0
+                f = torch.empty(q * lat.n, device="cuda", dtype=dt)
+                lat.observe(force, f=f)
+                results[(pitch, nodes, threads, lat.pz)] = f.cpu().numpy()
+        ref = results[(False, 1, 256, shape[2])]
+        assert any(k[0] and k[1] > 1 for k in results)
+        for k, v in results.items():
+            assert np.array_equal(v, ref), (shape, k, np.abs(v - ref).max())
