@@ -87,6 +87,7 @@ class LbmParticles(ctypes.Structure):
         ("inertia", ctypes.c_void_p),
         ("rou", ctypes.c_void_p),
         ("fp64", ctypes.c_int32),
+        ("extreme", ctypes.c_void_p),
     ]
 
 
@@ -118,6 +119,9 @@ SIGNATURES = {
     "ibm_spread": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P, _P]),
     "ibm_spread_noalloc": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P]),
     "rigid_update_markers": (I, [_PART, _P]),
+    "ibm_interpolate_wall": (I, [_LAT, _P, _FORCE, _P, _PART, F, F, ctypes.c_int32, _P, _P]),
+    "rigid_step": (I, [_PART, F, F, F, _P]),
+    "rigid_extremes": (I, [_PART, _P]),
     "lbm_debug_set_wait_limit": (None, [ctypes.c_int64]),
     "lbm_last_error": (ctypes.c_char_p, []),
     "lbm_version": (ctypes.c_char_p, []),

@@ -125,7 +125,48 @@ struct InterpArgs {
   int step;
   unsigned *status;
   StepPlanes planes;   // pull sources of fa (interior rows)
+  int wall;            // apply the wall spring at the extreme markers
+  float size[3];       // wall positions: nodes - 1 per axis
+  float dx;
 };
+
+// Wall spring of LBMD3.particle_to_wall (lbm/lbm3d.py:121-167) for marker m
+// of particle pi, whose force after interpolation is lf: k0 = 300 times
+// (1 - distance / (2 dx)), clamped at 0, along the wall normal, at the six
+// extreme markers `ext` (least x, y, z, greatest x, y, z); the reference's
+// indexed += reads all six old forces and the last of duplicate entries
+// wins; nothing happens when all six distances give 0.
+template <typename R>
+__device__ __forceinline__ void wall_spring(const PView<R> &P, const int32_t *ext, int m, int pi,
+                                            const float size[3], float dx, R lf[3]) {
+  const int m0 = P.offset[pi], m1 = P.offset[pi + 1];
+  bool valid = m1 > m0;
+  for (int k = 0; k < 6; ++k) valid = valid && ext[k] >= m0 && ext[k] < m1;
+  if (!valid) return;
+  bool mine = false;
+  for (int k = 0; k < 6; ++k) mine = mine || ext[k] == m;
+  if (!mine) return;
+  const R k0 = R(300);
+  R d[6], dmax = R(0);
+  for (int k = 0; k < 6; ++k) {
+    const R c = P.lx[3 * ext[k] + (k % 3)];
+    const R b = k < 3 ? R(0) : (R)size[k - 3];
+    d[k] = fmax(k0 * (R(1) - fabs(c - b) / (R(2) * (R)dx)), R(0));
+    dmax = fmax(dmax, d[k]);
+  }
+  if (dmax == R(0)) return;
+  R out[3] = {lf[0], lf[1], lf[2]};
+  for (int k = 0; k < 6; ++k) {
+    if (ext[k] != m) continue;
+    for (int c = 0; c < 3; ++c) {
+      const R nrm = (c == k % 3) ? (k < 3 ? R(1) : R(-1)) : R(0);
+      out[c] = lf[c] + nrm * d[k];
+    }
+  }
+  lf[0] = out[0];
+  lf[1] = out[1];
+  lf[2] = out[2];
+}
 
 template <int Q, int S>
 __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
@@ -187,11 +228,15 @@ __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
   const R wx = P.cw[3 * pi], wy = P.cw[3 * pi + 1], wz = P.cw[3 * pi + 2];
   const R v[3] = {P.cu[3 * pi] + (wy * rz - wz * ry), P.cu[3 * pi + 1] + (wz * rx - wx * rz),
                   P.cu[3 * pi + 2] + (wx * ry - wy * rx)};
+  R lf[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     P.lu[3 * m + k] = v[k];
-    P.lF[3 * m + k] = (R(2) * lrho) * (v[k] - lus) / (R)a.dt;
+    lf[k] = (R(2) * lrho) * (v[k] - lus) / (R)a.dt;
   }
+  if (a.wall) wall_spring<R>(P, a.p.extreme + 6 * pi, m, pi, a.size, a.dx, lf);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) P.lF[3 * m + k] = lf[k];
   P.lrou[m] = lrho;
 }
 
@@ -488,6 +533,181 @@ __global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles p
     for (int k = 0; k < 3; ++k) p.angle[3 * pi + k] = ang[k];
 }
 
+// ---------------------------------------------------------------------------
+// The six extreme markers of one particle (block per particle, kRigidThreads
+// threads): argmin x, y, z then argmax x, y, z of lx, first index on ties --
+// the markers LBMD3.particle_to_wall acts on (lbm/lbm3d.py:121-167).
+// Thread 0 receives them in ext.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void block_extremes(const PView<R> &P, int m0, int m1,
+                                               R (*s_v)[kRigidThreads / 32],
+                                               int (*s_i)[kRigidThreads / 32], int ext[6]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  R v[6];
+  int id[6];
+  for (int k = 0; k < 3; ++k) {
+    v[k] = R(INFINITY);
+    v[k + 3] = -R(INFINITY);
+    id[k] = id[k + 3] = 0x7fffffff;
+  }
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    for (int k = 0; k < 3; ++k) {
+      const R c = P.lx[3 * m + k];
+      argext_merge(v[k], id[k], c, m, true);
+      argext_merge(v[k + 3], id[k + 3], c, m, false);
+    }
+  }
+  for (int k = 0; k < 6; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const R v2 = __shfl_xor_sync(0xffffffffu, v[k], o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, id[k], o);
+      argext_merge(v[k], id[k], v2, i2, k < 3);
+    }
+    if (lane == 0) {
+      s_v[k][wid] = v[k];
+      s_i[k][wid] = id[k];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 6; ++k) {
+      R bv = s_v[k][0];
+      int bi = s_i[k][0];
+      for (int w = 1; w < kRigidThreads / 32; ++w) argext_merge(bv, bi, s_v[k][w], s_i[k][w], k < 3);
+      ext[k] = bi;
+    }
+  }
+  __syncthreads();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kRigidThreads) k_extremes(const lbm_particles pt) {
+  const PView<R> P = pview<R>(pt);
+  const int pi = blockIdx.x;
+  __shared__ R s_v[6][kRigidThreads / 32];
+  __shared__ int s_i[6][kRigidThreads / 32];
+  int ext[6];
+  block_extremes<R>(P, P.offset[pi], P.offset[pi + 1], s_v, s_i, ext);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 6; ++k) pt.extreme[6 * pi + k] = ext[k];
+}
+
+// Rigid update + marker transform + extremes of the new positions, one block
+// per particle: the RIGID_UPDATE part of k_rigid, then k_markers' rotation,
+// with the same arithmetic and summation order (so the same results).
+template <typename R>
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a) {
+  const PView<R> P = pview<R>(a.p);
+  const int pi = blockIdx.x;
+  const int m0 = P.offset[pi], m1 = P.offset[pi + 1];
+  __shared__ double s_sum[3][kRigidThreads / 32];
+  __shared__ R s_cx[3], s_cw[3];
+  __shared__ R s_v[6][kRigidThreads / 32];
+  __shared__ int s_i[6][kRigidThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+
+  // -- cF = sum(-lF lm) + (1 - rho_p / rho_f) mass [gl, 0, 0]   (float64 sums)
+  double sf[3] = {0.0, 0.0, 0.0};
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    const double lm = P.lm[m];
+    for (int k = 0; k < 3; ++k) sf[k] += -(double)P.lF[3 * m + k] * lm;
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) sf[k] += __shfl_xor_sync(0xffffffffu, sf[k], o);
+    if (lane == 0) s_sum[k][wid] = sf[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const R mass = P.mass[pi];
+    const R buoy = (R)(1.0 - (double)P.rou[pi] / (double)a.rouf) * mass;
+    for (int k = 0; k < 3; ++k) {
+      double t = 0.0;
+      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
+      const R cf = (R)t + (k == 0 ? buoy * (R)a.gl : R(0));
+      P.cF[3 * pi + k] = cf;
+      const R cu = P.cu[3 * pi + k] + cf / mass * (R)a.dt;
+      P.cu[3 * pi + k] = cu;
+      const R cx = P.cx[3 * pi + k] + cu * (R)a.dt;
+      P.cx[3 * pi + k] = cx;
+      s_cx[k] = cx;
+    }
+  }
+  __syncthreads();
+
+  // -- cT = -sum((lx - cx) x lF lm)  with the new cx   (float64 sums)
+  double st[3] = {0.0, 0.0, 0.0};
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    const double rx = (double)(P.lx[3 * m] - s_cx[0]);
+    const double ry = (double)(P.lx[3 * m + 1] - s_cx[1]);
+    const double rz = (double)(P.lx[3 * m + 2] - s_cx[2]);
+    const double fx = P.lF[3 * m], fy = P.lF[3 * m + 1], fz = P.lF[3 * m + 2];
+    const double lm = P.lm[m];
+    st[0] += (ry * fz - rz * fy) * lm;
+    st[1] += (rz * fx - rx * fz) * lm;
+    st[2] += (rx * fy - ry * fx) * lm;
+  }
+  __syncthreads();
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) st[k] += __shfl_xor_sync(0xffffffffu, st[k], o);
+    if (lane == 0) s_sum[k][wid] = st[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 3; ++k) {
+      double t = 0.0;
+      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
+      const R ct = -(R)t;
+      P.cT[3 * pi + k] = ct;
+      const R cw = P.cw[3 * pi + k] + R(0.1) * ct * (R)a.dt / P.inertia[3 * pi + k];
+      P.cw[3 * pi + k] = cw;
+      s_cw[k] = cw;
+    }
+  }
+  __syncthreads();   // every thread has read lx for the torque; cw is final
+
+  // -- angle += cw; lx = R(angle) X0 + cx   (particle/coord.py:87-108)
+  double v[3];
+  R ang[3], c[3];
+  for (int k = 0; k < 3; ++k) {
+    ang[k] = P.angle[3 * pi + k] + s_cw[k];
+    v[k] = ang[k];
+    c[k] = s_cx[k];
+  }
+  const double th = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  double sc;
+  if (th <= 1e-3) {
+    const double t2 = th * th;
+    sc = 0.5 - t2 / 48.0 + t2 * t2 / 3840.0;
+  } else {
+    sc = sin(0.5 * th) / th;
+  }
+  double x = sc * v[0], y = sc * v[1], z = sc * v[2], w = cos(0.5 * th);
+  const double nq = sqrt(x * x + y * y + z * z + w * w);
+  x /= nq;
+  y /= nq;
+  z /= nq;
+  w /= nq;
+  const double M[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w),     2 * (x * z + y * w),
+                       2 * (x * y + z * w),     1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                       2 * (x * z - y * w),     2 * (y * z + x * w),     1 - 2 * (x * x + y * y)};
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    const double X = P.lagrange[3 * m], Y = P.lagrange[3 * m + 1], Z = P.lagrange[3 * m + 2];
+    for (int k = 0; k < 3; ++k) {
+      const double r = M[3 * k] * X + M[3 * k + 1] * Y + M[3 * k + 2] * Z;
+      P.lx[3 * m + k] = (R)r + c[k];
+    }
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) P.angle[3 * pi + k] = ang[k];
+  if (a.p.extreme == nullptr) return;
+  __syncthreads();   // the new positions are written
+  int ext[6];
+  block_extremes<R>(P, m0, m1, s_v, s_i, ext);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 6; ++k) a.p.extreme[6 * pi + k] = ext[k];
+}
+
 template <int Q>
 struct RunInterp {
   static int run(const InterpArgs &a, int storage, cudaStream_t s) {
@@ -717,6 +937,105 @@ int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, fl
   return lat->storage == LBM_STORAGE_FP64
              ? spread_launch<double>(a, mode, pt->n_markers, s, "ibm_spread")
              : spread_launch<float>(a, mode, pt->n_markers, s, "ibm_spread");
+}
+
+int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                         const float *face_rho_in, const lbm_particles *pt, float dt, float dx,
+                         int32_t step, uint32_t *status, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if ((rc = check_particles(pt, "ibm_interpolate_wall"))) return rc;
+  if (!(dt > 0.f)) {
+    set_error("ibm_interpolate_wall: dt must be positive");
+    return LBM_ERR_INVALID;
+  }
+  if (fa == nullptr) {
+    set_error("ibm_interpolate_wall: needs the post-collision populations");
+    return LBM_ERR_INVALID;
+  }
+  if (any_face(lat, LBM_BC_NON_EQUILIBRIUM)) {
+    set_error("ibm_interpolate_wall: NON_EQUILIBRIUM faces need the u / rho fields");
+    return LBM_ERR_UNSUPPORTED;
+  }
+  if (any_face(lat, LBM_BC_WALL_WITH_SPEED) && face_rho_in == nullptr) {
+    set_error("ibm_interpolate_wall: WALL_WITH_SPEED faces need face_rho_in");
+    return LBM_ERR_INVALID;
+  }
+  if ((rc = check_precision(lat, pt, "ibm_interpolate_wall"))) return rc;
+  if (pt->n_markers == 0) return LBM_OK;
+  if (pt->extreme == nullptr) {
+    set_error("ibm_interpolate_wall: the particles' extreme markers are required");
+    return LBM_ERR_INVALID;
+  }
+  InterpArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = make_geom(lat);
+  a.fa = fa;
+  fill_step_planes(a.g, lat->q, lat->storage, fa, nullptr, a.planes);
+  if (force != nullptr) {
+    for (int k = 0; k < 3; ++k) a.go[k] = force->old_uniform[k];
+    a.fol_old = force->old_field;
+  }
+  a.face_rho_in = face_rho_in;
+  a.p = *pt;
+  a.dt = dt;
+  a.step = step;
+  a.status = status;
+  a.wall = 1;
+  a.size[0] = (float)(lat->nx - 1);
+  a.size[1] = (float)(lat->ny - 1);
+  a.size[2] = (float)(lat->nz - 1);
+  a.dx = dx;
+  switch (lat->q) {
+    case 13: return RunInterp<13>::run(a, lat->storage, (cudaStream_t)stream);
+    case 15: return RunInterp<15>::run(a, lat->storage, (cudaStream_t)stream);
+    case 19: return RunInterp<19>::run(a, lat->storage, (cudaStream_t)stream);
+    default: return RunInterp<27>::run(a, lat->storage, (cudaStream_t)stream);
+  }
+}
+
+int rigid_step(const lbm_particles *pt, float dt, float gl, float rouf, void *stream) {
+  int rc = check_particles(pt, "rigid_step");
+  if (rc) return rc;
+  if (!(dt > 0.f)) {
+    set_error("Time step must be positive");
+    return LBM_ERR_INVALID;
+  }
+  if (!(rouf > 0.f)) {
+    set_error("Fluid density must be positive");
+    return LBM_ERR_INVALID;
+  }
+  if (pt->n_particles == 0) return LBM_OK;
+  RigidArgs a;
+  memset(&a, 0, sizeof(a));
+  a.p = *pt;
+  a.what = RIGID_UPDATE;
+  a.dt = dt;
+  a.dx = 1.f;
+  a.gl = gl;
+  a.rouf = rouf;
+  if (pt->fp64)
+    k_rigid_step<double><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
+  else
+    k_rigid_step<float><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
+  LBM_LAUNCH_CHECK("rigid_step");
+  return LBM_OK;
+}
+
+int rigid_extremes(const lbm_particles *pt, void *stream) {
+  int rc = check_particles(pt, "rigid_extremes");
+  if (rc) return rc;
+  if (pt->n_particles == 0) return LBM_OK;
+  if (pt->extreme == nullptr) {
+    set_error("rigid_extremes: no output array (extreme)");
+    return LBM_ERR_INVALID;
+  }
+  if (pt->fp64)
+    k_extremes<double><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
+  else
+    k_extremes<float><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
+  LBM_LAUNCH_CHECK("rigid_extremes");
+  return LBM_OK;
 }
 
 int rigid_update_markers(const lbm_particles *pt, void *stream) {

@@ -5,9 +5,11 @@
 
 * no particles -- one kernel per step (stream, moments, forcing, moments,
   collide of ``lbm/base.py:159-175`` plus the next step's ``cul_equ``);
-* particles -- interpolation (fused with the moment pass it reads), wall
-  spring + Newton-Euler update, spreading, the fused step, marker update:
-  five launches per step, in the reference's phase order.
+* particles -- interpolation (fused with the moment pass it reads and the
+  wall spring), spreading, the Newton-Euler update fused with the marker
+  update, the fused step: four C-ABI calls per step.  The particle update
+  runs before the flow step (the reference runs it after): neither reads
+  the other's results, so the state is the reference's.
 
 NON_EQUILIBRIUM faces, or ``"fused": false`` in the config, run the
 reference's call sequence instead (``_compute_flow`` ->
@@ -456,29 +458,32 @@ class LBMD3(LBMBase):
                 "keep": (F_old, F_new, C_old, C_new), "ibm": True}
         if not launch:
             return plan
+        dt = float(self.config.dt)
         if parts:
             sw = self.particle_swarm
+            sw.ensure_extremes()
             st = ctypes.byref(sw.struct())
             f_int = make_force(old_uniform=g_old, old_field=F_old)
-            call("ibm_interpolate", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]), ctypes_ref(f_int),
-                 ptr(lat.face_rho[lat.cur]), None, None, st, float(self.config.dt),
+            # flow_to_lagrange and particle_to_wall in one launch
+            call("ibm_interpolate_wall", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]),
+                 ctypes_ref(f_int), ptr(lat.face_rho[lat.cur]), st, dt, float(self.config.dx),
                  int(self.step), ptr(self._status_ibm), s)
-            call("rigid_wall_and_update", ctypes_ref(lat.desc), st,
-                 _lib.RIGID_WALL | _lib.RIGID_UPDATE, float(self.config.dt),
-                 float(self.config.dx), float(self.config.flow_config.gl), 1.0, s)
         mode = 0 if self.config.ibm_mode == "reference" else 1
         sw_struct = self.particle_swarm.struct() if parts else _empty_particles()
         call("ibm_spread", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode, ptr(F_new),
              ptr(C_new), ptr(self._owner), s)
+        if parts:
+            # update_from_lar and Particle.update (with the next step's wall
+            # markers) in one launch: nothing after spreading reads the old
+            # positions, and the flow step does not read particle state
+            call("rigid_step", st, dt, float(self.config.flow_config.gl), 1.0, s)
+            sw.ext_valid = True
         return plan
 
     def fused_finish(self, plan):
-        """Everything of a fused step after the step kernel: the marker update
-        and the force-buffer swap."""
+        """Everything of a fused step after the step kernel: the force-buffer
+        swap (the particle update ran with the IBM launches)."""
         if plan["ibm"]:
-            if self.particle_swarm.particles:
-                call("rigid_update_markers", ctypes.byref(self.particle_swarm.struct()),
-                     self._stream())
             self._fi ^= 1
         self._g_old = plan["g_new"]
 

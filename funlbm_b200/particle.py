@@ -261,6 +261,9 @@ class Particle:
                 t.copy_(v.reshape(t.shape))
             else:
                 self.__dict__["_t"][key] = v.clone()
+            sw = self.__dict__.get("_swarm")
+            if key == "lx" and sw is not None:
+                sw.ext_valid = False
             return
         object.__setattr__(self, key, value)
 
@@ -281,6 +284,7 @@ class Particle:
         self._require_swarm()
         sw = self._swarm
         call("rigid_update_markers", ctypes.byref(sw.single(self._index)), sw.stream())
+        sw.ext_valid = False
 
     def _require_swarm(self):
         if self._swarm is None:
@@ -456,6 +460,11 @@ class ParticleSwarm:
             p.coord._center = self.cx[i]
             p._swarm = self
             p._index = i
+        # the wall spring's six extreme markers of each particle (kept by
+        # rigid_step; recomputed by rigid_extremes when positions changed
+        # any other way)
+        self.extreme = torch.zeros((max(P, 1), 6), dtype=torch.int32, device=dev)
+        self.ext_valid = False
         self._singles = {}
         self._struct = self._make_struct(0, P, offs, self.owner, self.offsets)
         self._packed = True
@@ -483,6 +492,7 @@ class ParticleSwarm:
         s.inertia = at(self.inertia, p0)
         s.rou = at(self.rou, p0)
         s.fp64 = 1 if self.dtype == torch.float64 else 0
+        s.extreme = self.extreme.data_ptr() + p0 * 6 * 4
         return s
 
     def struct(self):
@@ -508,6 +518,13 @@ class ParticleSwarm:
         if not self.particles:
             return
         call("rigid_update_markers", ctypes.byref(self.struct()), self.stream())
+        self.ext_valid = False
+
+    def ensure_extremes(self):
+        """Make `extreme` hold the extreme markers of the current positions."""
+        if self.particles and not self.ext_valid:
+            call("rigid_extremes", ctypes.byref(self.struct()), self.stream())
+            self.ext_valid = True
 
     def save_particle(self):
         pass
@@ -519,6 +536,7 @@ class ParticleSwarm:
     def load_checkpoint(self, group=None, *args, **kwargs):
         for i, particle in enumerate(self.particles):
             particle.load_checkpoint(group.get("particle_%06d" % i), *args, **kwargs)
+        self.ext_valid = False
 
 
 def create_particle_swarm(configs: List[ParticleConfig] = (), device="cuda", dtype=torch.float32,

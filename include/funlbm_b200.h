@@ -232,6 +232,11 @@ typedef struct lbm_particles {
   const float *rou;              /* [n_particles] particle density            */
   int32_t fp64;                  /* 1: every float array above holds float64  */
                                  /* (particles of an LBM_STORAGE_FP64 lattice) */
+  int32_t *extreme;              /* [n_particles][6] markers of least x, y, z */
+                                 /* and greatest x, y, z (first on ties), the  */
+                                 /* wall spring's markers; kept by rigid_step  */
+                                 /* / rigid_extremes, read by                  */
+                                 /* ibm_interpolate_wall (NULL otherwise)      */
 } lbm_particles;
 
 /* LBMD3.flow_to_lagrange (lbm/lbm3d.py:66-100) fused with the moment pass
@@ -287,6 +292,30 @@ int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, fl
 #define LBM_SPREAD_NOALLOC_MAX_NODES (1 << 22)
 int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
                        uint8_t *chunks, void *stream);
+
+/* LBMD3.flow_to_lagrange fused with LBMD3.particle_to_wall
+ * (lbm/lbm3d.py:66-167): the interpolation of ibm_interpolate from the
+ * post-collision populations `fa`, and the wall spring of
+ * rigid_wall_and_update(RIGID_WALL) applied to the six extreme markers of each
+ * particle as their forces are written (pt->extreme must hold the extremes of
+ * the current positions: rigid_step keeps it, rigid_extremes recomputes it).
+ * `dx` is the spring's length scale.  Same results as the two calls. */
+int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                         const float *face_rho_in, const lbm_particles *pt, float dt, float dx,
+                         int32_t step, uint32_t *status, void *stream);
+
+/* Particle.update_from_lar then Particle.update (particle/base/base.py:120-156,
+ * particle/coord.py:87-108) for all particles in one launch -- the rigid
+ * update of rigid_wall_and_update(RIGID_UPDATE) followed by the marker
+ * transform of rigid_update_markers -- and the six extreme markers of the new
+ * positions into pt->extreme (when not NULL) for the next step's wall spring.
+ * The spring itself is not applied here (ibm_interpolate_wall does it).
+ * Same results as the two calls. */
+int rigid_step(const lbm_particles *pt, float dt, float gl, float rouf, void *stream);
+
+/* The six extreme markers of the current positions into pt->extreme
+ * (the argmin / argmax of lbm/lbm3d.py:121-167). */
+int rigid_extremes(const lbm_particles *pt, void *stream);
 
 /* Particle.update + Coordinate.update/cul_point (particle/base/base.py:153-156,
  * particle/coord.py:87-108): angle += cw; lx = R(angle) lagrange + cx, with the

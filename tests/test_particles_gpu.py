@@ -203,3 +203,74 @@ def test_run_with_graphs_matches_eager():
             assert len(lbm._graphs) >= 2          # before and after step 100
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp64"])
+def test_fused_particle_calls_match_separate_calls(storage):
+    """ibm_interpolate_wall + rigid_step (the driver's calls) against
+    ibm_interpolate + rigid_wall_and_update(RIGID_WALL | RIGID_UPDATE) +
+    rigid_update_markers (one reference function each) on the same state:
+    forces, particle state, rotation vectors and new marker positions agree
+    bit for bit, and the extremes rigid_step leaves are those of the new
+    positions.  Particles touch the walls (the spring acts) and one has
+    duplicate extreme markers (a tiny sphere)."""
+    import ctypes
+
+    from funlbm_b200 import _lib
+    from funlbm_b200._lib import call, ptr
+    from funlbm_b200.lattice import ctypes_ref, make_force
+
+    dt = torch.float64 if storage == "fp64" else torch.float32
+    parts = [{"type": "sphere", "r": 3, "rou": 1.4, "coord": {"center": [2.2, 8.0, 9.1]}},
+             {"type": "ellipsoid", "a": 3, "b": 2, "c": 2.5, "rou": 0.7,
+              "coord": {"center": [14.5, 13.3, 1.6], "alpha": 0.3, "beta": -0.5, "gamma": 0.2}},
+             {"type": "sphere", "r": 1, "rou": 1.1, "coord": {"center": [9.0, 6.0, 9.0]}}]
+    states = []
+    for variant in ("separate", "fused"):
+        lbm = LBMD3_with(parts, storage)
+        lat = lbm.flow.lattice
+        sw = lbm.particle_swarm
+        sw.update()                               # markers on the bodies
+        g = torch.Generator(device="cpu").manual_seed(3)
+        sw.cu.copy_((0.01 * torch.randn(sw.cu.shape, generator=g)).to(dt))
+        sw.cw.copy_((0.01 * torch.randn(sw.cw.shape, generator=g)).to(dt))
+        st = ctypes.byref(sw.struct())
+        s = lat.stream()
+        force = make_force()
+        status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        if variant == "separate":
+            call("ibm_interpolate", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]), ctypes_ref(force),
+                 ptr(lat.face_rho[lat.cur]), None, None, st, 1.0, 5, ptr(status), s)
+            call("rigid_wall_and_update", ctypes_ref(lat.desc), st,
+                 _lib.RIGID_WALL | _lib.RIGID_UPDATE, 1.0, 1.0, 1e-3, 1.0, s)
+            call("rigid_update_markers", st, s)
+            ext = None
+        else:
+            call("rigid_extremes", st, s)
+            call("ibm_interpolate_wall", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]),
+                 ctypes_ref(force), ptr(lat.face_rho[lat.cur]), st, 1.0, 1.0, 5, ptr(status), s)
+            call("rigid_step", st, 1.0, 1e-3, 1.0, s)
+            ext = sw.extreme.cpu().numpy()[:len(parts)]
+        torch.cuda.synchronize()
+        states.append([t.cpu().numpy().copy() for t in
+                       (sw.lF, sw.lu, sw.cF, sw.cT, sw.cx, sw.cu, sw.cw, sw.angle, sw.lx)])
+        if ext is not None:
+            lx = sw.lx.cpu().numpy()
+            offs = sw._offsets_host
+            for i in range(len(parts)):
+                seg = lx[offs[i]:offs[i + 1]]
+                want = np.concatenate([np.argmin(seg, 0), np.argmax(seg, 0)]) + offs[i]
+                assert np.array_equal(ext[i], want), i
+    spring = np.abs(states[1][0] - states[0][0]).max()
+    for k, (a, b) in enumerate(zip(*states)):
+        assert np.array_equal(a, b), (k, np.abs(a - b).max(), spring)
+
+
+def LBMD3_with(parts, storage):
+    from funlbm_b200.lbm import LBMD3
+
+    lbm = LBMD3(config=lbm_config(19, (16, 16, 18), 0.1, [1200] * 6, particles=parts, gl=1e-3,
+                                  storage=storage))
+    init_with(lbm, None)
+    run(lbm, 3)
+    return lbm
