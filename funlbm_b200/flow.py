@@ -293,6 +293,8 @@ class FlowD3(Flow):
             return
         lat = self._lat
         force, fields = self._last_force
+        if self._f is None:        # released while stepping in the fused form
+            self._f = torch.empty((self.q, self.n), device=self.device, dtype=lat.real_dtype)
         lat.observe(force, f=self._f, rho=self._rou, u=self._u)
         self._p = self._rou / 3.0
         new_field, new_uniform = fields
@@ -319,6 +321,7 @@ class FlowD3(Flow):
                 self._fp64_only_fused("entering the fused form from a stepped state")
             lat.allocate()
             lat.init(self._f)
+            self._release_reference_populations()
             self._mode = "fused"
             self._obs_valid = False
             return
@@ -330,8 +333,17 @@ class FlowD3(Flow):
         del post
         if lat.needs_face_rho:
             lat.face_rho[lat.cur].copy_(face_planes(self._rou.view(self.shape)))
+        self._release_reference_populations()
         self._mode = "fused"
         self._obs_valid = False
+
+    def _release_reference_populations(self):
+        """The fused form keeps the state in the lattice buffers: drop the
+        reference-form populations (f, feq and the streaming copy, 4-12 bytes
+        per direction and node); observing the state allocates f again."""
+        self._f = None
+        self._f2 = None
+        self._feq = None
 
     def fused_step(self, force, new_field=None, new_uniform=(0.0, 0.0, 0.0), keep=()):
         """One fused step on the lattice buffers (caller prepared `force`)."""

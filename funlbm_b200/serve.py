@@ -5,18 +5,22 @@
 and an arrival time -- and runs them with continuous batching:
 
 * **admission** -- a request is admitted as soon as it has arrived, a slot is
-  free and its estimated device memory fits in the HBM budget; requests that
-  arrive while others run join at the next chunk boundary, and finished ones
-  free their slot and memory at once;
+  free and its estimated device memory (its population buffers, moment and
+  force fields and IBM buffers, plus room for the copy made while it is
+  built) fits in the HBM budget; finished requests free their slot and
+  memory at once;
 * **resident state** -- each admitted request keeps its populations,
   particle state and IBM buffers on the device until it finishes;
-* **one launch per class per step** -- the fused step kernels of every
-  active lattice of the same (velocity set, storage, nodes per thread) run
-  in one multi-lattice launch (``lbm_flow_step_batch``); the particle
-  kernels of each lattice are issued around it in the reference's order;
-* **captured CUDA graphs** -- while the active set is unchanged, two steps of
-  the whole active set are captured once and replayed, so a step costs one
-  graph launch instead of dozens of kernel launches from Python.
+* **overlapped execution (mode "streams", the default)** -- every request
+  runs on the least-loaded stream of a pool, from its own captured CUDA
+  graphs of up to 32 steps, enqueued in chunks a bounded distance ahead of
+  the device, so the requests' kernels overlap on the GPU while requests
+  join and leave;
+* **multi-lattice launches (mode "batched")** -- all active lattices of one
+  (velocity set, storage, nodes per thread) advance in one multi-lattice
+  launch per step (``lbm_flow_step_batch``), the particle kernels of each
+  lattice issued around it, two steps of the whole active set captured as
+  one graph and recaptured when the set changes.
 
 Each request's result (final rho, u and particle state) is the same as when
 it runs alone through ``LBMD3.run_step``: the batched kernel runs the same
@@ -34,7 +38,7 @@ import torch
 
 from . import _lib
 from ._lib import call, ptr
-from .lattice import BYTES, ctypes_ref
+from .lattice import REAL_DTYPE, Lattice, ctypes_ref
 
 _ids = itertools.count()
 
@@ -62,19 +66,34 @@ def _shape_of(cfg):
     return tuple(int(s) + 1 for s in size)
 
 
-def estimate_bytes(cfg):
-    """Device memory one request holds while admitted: population buffers,
-    the reference-form tensors kept for observation, moments / force fields
-    and, with particles, the IBM buffers."""
+def _q_storage(cfg):
     flow = cfg.get("flow") or {}
     q = int(str(flow.get("param_type") or "D3Q19")[3:])
     storage = ((flow.get("precision") or {}).get("storage")) or flow.get("storage") or "fp32"
+    return q, storage
+
+
+def estimate_bytes(cfg):
+    """Device memory one request holds while it steps: the two population
+    buffers (rows pitched), the moments / force fields kept for observation
+    and, with particles, the IBM buffers.  The reference-form populations
+    exist only while a request enters the fused form and while its result is
+    read (transient_bytes)."""
+    q, storage = _q_storage(cfg)
     X, Y, Z = _shape_of(cfg)
     n = X * Y * Z
-    pops = 2 * q * n * BYTES[storage] + 2 * 4 * q * n      # A/B + f and feq (float32)
-    fields = (3 + 1 + 1 + 3) * 4 * n                         # u, rho, p, FOL
+    pops = Lattice.bytes_needed(q, (X, Y, Z), storage)
+    fields = (3 + 1 + 1 + 3) * REAL_DTYPE[storage].itemsize * n     # u, rho, p, FOL
     ibm = (2 * 12 + 4) * n + 2 * (n // 32 + 1) if cfg.get("particles") else 0
     return int(pops + fields + ibm + (8 << 20))
+
+
+def transient_bytes(cfg):
+    """Extra device memory while a request enters the fused form or its
+    result is read: the reference-form populations and one copy of them."""
+    q, storage = _q_storage(cfg)
+    X, Y, Z = _shape_of(cfg)
+    return int(2 * q * X * Y * Z * REAL_DTYPE[storage].itemsize)
 
 
 class _Slot:
@@ -152,7 +171,7 @@ class LBMServer:
 
     # -- queue ---------------------------------------------------------------
     def submit(self, req: Request):
-        if estimate_bytes(req.config) > self.budget:
+        if estimate_bytes(req.config) + transient_bytes(req.config) > self.budget:
             raise ValueError("request %d needs more device memory than the whole budget" % req.rid)
         self.queue.append(req)
         self.queue.sort(key=lambda r: r.arrival)
@@ -165,7 +184,8 @@ class LBMServer:
             if req.arrival > now:
                 break
             nbytes = estimate_bytes(req.config)
-            if self.used + nbytes > self.budget:
+            # room for the request and for its transient while it is built
+            if self.used + nbytes + transient_bytes(req.config) > self.budget:
                 i += 1                      # first fit: a smaller request may go ahead
                 continue
             self.queue.pop(i)
