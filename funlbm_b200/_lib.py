@@ -121,6 +121,8 @@ SIGNATURES = {
     "rigid_update_markers": (I, [_PART, _P]),
     "ibm_interpolate_wall": (I, [_LAT, _P, _FORCE, _P, _PART, F, F, ctypes.c_int32, _P, _P]),
     "rigid_step": (I, [_PART, F, F, F, _P]),
+    "ibm_spread_tiled_scratch_bytes": (ctypes.c_size_t, [_LAT, ctypes.c_int32]),
+    "ibm_spread_tiled": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),
     "rigid_extremes": (I, [_PART, _P]),
     "lbm_debug_set_wait_limit": (None, [ctypes.c_int64]),
     "lbm_last_error": (ctypes.c_char_p, []),

@@ -473,6 +473,144 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Tiled spreading: the lattice is cut into 8 x 8 x 8-node tiles.  k_spread_bin
+// (thread = marker x stencil slot, as k_spread) takes each marker's
+// normalising weight sum and lists the marker under every tile its stencil
+// box touches (at most 8).  k_spread_tile (block = tile) then resolves the
+// tile entirely in shared memory: reference mode takes the last writer of
+// every node (largest marker index, the reference's loop order) with
+// shared-memory atomicMax and writes each claimed node once; accumulate mode
+// sums the contributions in shared memory and stores each node once.  No
+// global atomics touch the field, and no global claim array is needed.
+// ---------------------------------------------------------------------------
+constexpr int kTile = 8;
+constexpr int kTileNodes = kTile * kTile * kTile;
+constexpr int kTileCap = 512;      // markers listed per tile; more: the tile scans all markers
+
+struct TileArgs {
+  Geom g;
+  lbm_particles p;
+  void *field;        // [n][3] in the particles' arithmetic type
+  uint8_t *chunks;
+  int *tile_count;    // [ntiles], zero between calls
+  int *tile_list;     // [ntiles][kTileCap]
+  void *wsum;         // [n_markers] normalising weight sums
+  int tx, ty, tz;     // tiles per axis
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kIbmThreads) k_spread_bin(const TileArgs a) {
+  __shared__ R sh[1][kMarkersPerBlock * 2];
+  const PView<R> P = pview<R>(a.p);
+  const int mk = threadIdx.x / kStencil, slot = threadIdx.x % kStencil;
+  const int m = blockIdx.x * kMarkersPerBlock + mk;
+  const bool live = m < a.p.n_markers;
+  R l[3] = {R(0), R(0), R(0)};
+  int x = 0, y = 0, z = 0;
+  R w = R(0);
+  bool in_box = false;
+  if (live) {
+    l[0] = P.lx[3 * m];
+    l[1] = P.lx[3 * m + 1];
+    l[2] = P.lx[3 * m + 2];
+    in_box = stencil_slot(a.g, l, slot, x, y, z, w);
+  }
+  R W[1] = {in_box ? w : R(0)};
+  stencil_sum<1>(W, sh, slot, mk);
+  if (!live || slot != 0) return;
+  static_cast<R *>(a.wsum)[m] = W[0];
+  int lo[3], hi[3];
+  box_axis(l[0], a.g.nx - 1, lo[0], hi[0]);
+  box_axis(l[1], a.g.ny - 1, lo[1], hi[1]);
+  box_axis(l[2], a.g.nz - 1, lo[2], hi[2]);
+  if (hi[0] <= lo[0] || hi[1] <= lo[1] || hi[2] <= lo[2]) return;
+  for (int i = lo[0] / kTile; i <= (hi[0] - 1) / kTile; ++i)
+    for (int j = lo[1] / kTile; j <= (hi[1] - 1) / kTile; ++j)
+      for (int k = lo[2] / kTile; k <= (hi[2] - 1) / kTile; ++k) {
+        const int t = (i * a.ty + j) * a.tz + k;
+        const int pos = atomicAdd(a.tile_count + t, 1);
+        if (pos < kTileCap) a.tile_list[(long long)t * kTileCap + pos] = m;
+      }
+}
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kTileNodes) k_spread_tile(const TileArgs a) {
+  __shared__ int s_owner[kTileNodes];
+  __shared__ R s_acc[MODE == 1 ? kTileNodes * 3 : 1];
+  const int t = blockIdx.x;
+  const int cnt = a.tile_count[t];
+  if (cnt == 0) return;
+  const PView<R> P = pview<R>(a.p);
+  const R *wsum = static_cast<const R *>(a.wsum);
+  R *field = static_cast<R *>(a.field);
+  const int ti = t / (a.ty * a.tz), tj = (t / a.tz) % a.ty, tk = t % a.tz;
+  const int ox = ti * kTile, oy = tj * kTile, oz = tk * kTile;
+  const int tid = threadIdx.x;
+  s_owner[tid] = -1;
+  if constexpr (MODE == 1) {
+    s_acc[3 * tid] = R(0);
+    s_acc[3 * tid + 1] = R(0);
+    s_acc[3 * tid + 2] = R(0);
+  }
+  __syncthreads();
+  const bool all = cnt > kTileCap;   // list overflowed: scan every marker
+  const long long pairs = (long long)(all ? a.p.n_markers : cnt) * kStencil;
+  for (long long pr = tid; pr < pairs; pr += kTileNodes) {
+    const int li = (int)(pr / kStencil), slot = (int)(pr % kStencil);
+    const int m = all ? li : a.tile_list[(long long)t * kTileCap + li];
+    const R l[3] = {P.lx[3 * m], P.lx[3 * m + 1], P.lx[3 * m + 2]};
+    int x, y, z;
+    R w;
+    if (!stencil_slot(a.g, l, slot, x, y, z, w)) continue;
+    const int dx = x - ox, dy = y - oy, dz = z - oz;
+    if (dx < 0 || dx >= kTile || dy < 0 || dy >= kTile || dz < 0 || dz >= kTile) continue;
+    const int local = (dx * kTile + dy) * kTile + dz;
+    if constexpr (MODE == 0) {
+      atomicMax(s_owner + local, m);
+    } else {
+      const R W = wsum[m];
+      const R wn = W > R(0) ? w / W : w;
+      const R lm = P.lm[m];
+      for (int k = 0; k < 3; ++k) atomicAdd(s_acc + 3 * local + k, (wn * P.lF[3 * m + k]) * lm);
+      s_owner[local] = 0;   // touched
+    }
+  }
+  __syncthreads();
+  const int x = ox + tid / (kTile * kTile), y = oy + (tid / kTile) % kTile, z = oz + tid % kTile;
+  const int m = s_owner[tid];
+  if (m >= 0 && x < a.g.nx && y < a.g.ny && z < a.g.nz) {
+    const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
+    a.chunks[idx >> 5] = 1;
+    if constexpr (MODE == 0) {
+      // the winner's weight at this node: its stencil slot of (x, y, z)
+      const R l[3] = {P.lx[3 * m], P.lx[3 * m + 1], P.lx[3 * m + 2]};
+      int lo[3], hi[3];
+      box_axis(l[0], a.g.nx - 1, lo[0], hi[0]);
+      box_axis(l[1], a.g.ny - 1, lo[1], hi[1]);
+      box_axis(l[2], a.g.nz - 1, lo[2], hi[2]);
+      const int slot = ((x - lo[0]) * 4 + (y - lo[1])) * 4 + (z - lo[2]);
+      int xs, ys, zs;
+      R w;
+      stencil_slot(a.g, l, slot, xs, ys, zs, w);
+      const R W = wsum[m];
+      const R wn = W > R(0) ? w / W : w;
+      const R lm = P.lm[m];
+      for (int k = 0; k < 3; ++k) field[3 * idx + k] = (wn * P.lF[3 * m + k]) * lm;
+    } else {
+      for (int k = 0; k < 3; ++k) field[3 * idx + k] = s_acc[3 * tid + k];
+    }
+  }
+  __syncthreads();
+  if (tid == 0) a.tile_count[t] = 0;    // ready for the next call
+}
+
+static void tile_dims(const Geom &g, int &tx, int &ty, int &tz) {
+  tx = (g.nx + kTile - 1) / kTile;
+  ty = (g.ny + kTile - 1) / kTile;
+  tz = (g.nz + kTile - 1) / kTile;
+}
+
+// ---------------------------------------------------------------------------
 // Marker update (particle/base/base.py:153-156, particle/coord.py:87-108):
 // angle += cw; R from the rotation vector (float64, through the unit
 // quaternion); lx = float32(R X0) + cx.  One block per particle.
@@ -1035,6 +1173,75 @@ int rigid_extremes(const lbm_particles *pt, void *stream) {
   else
     k_extremes<float><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(*pt);
   LBM_LAUNCH_CHECK("rigid_extremes");
+  return LBM_OK;
+}
+
+size_t ibm_spread_tiled_scratch_bytes(const lbm_lattice *lat, int32_t n_markers) {
+  if (lat == nullptr || n_markers < 0) return 0;
+  const Geom g = make_geom(lat);
+  int tx, ty, tz;
+  tile_dims(g, tx, ty, tz);
+  const size_t ntiles = (size_t)tx * ty * tz;
+  const size_t real = lat->storage == LBM_STORAGE_FP64 ? 8 : 4;
+  return ntiles * 4 + ntiles * kTileCap * 4 + (size_t)n_markers * real + 256;
+}
+
+int ibm_spread_tiled(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
+                     uint8_t *chunks, void *scratch, size_t scratch_bytes, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if ((rc = check_particles(pt, "ibm_spread_tiled"))) return rc;
+  if (mode != 0 && mode != 1) {
+    set_error("ibm_spread_tiled: mode must be 0 (reference) or 1 (accumulate)");
+    return LBM_ERR_INVALID;
+  }
+  if (field == nullptr || chunks == nullptr || scratch == nullptr) {
+    set_error("ibm_spread_tiled: field, chunks and scratch are required");
+    return LBM_ERR_INVALID;
+  }
+  if (scratch_bytes < ibm_spread_tiled_scratch_bytes(lat, pt->n_markers)) {
+    set_error("ibm_spread_tiled: scratch of %zu bytes, %zu needed", scratch_bytes,
+              ibm_spread_tiled_scratch_bytes(lat, pt->n_markers));
+    return LBM_ERR_INVALID;
+  }
+  if ((rc = check_precision(lat, pt, "ibm_spread_tiled"))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  TileArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = make_geom(lat);
+  a.p = *pt;
+  a.field = field;
+  a.chunks = chunks;
+  tile_dims(a.g, a.tx, a.ty, a.tz);
+  const long long ntiles = (long long)a.tx * a.ty * a.tz;
+  char *base = static_cast<char *>(scratch);
+  a.tile_count = reinterpret_cast<int *>(base);
+  a.tile_list = a.tile_count + ntiles;
+  const size_t off = ((size_t)(ntiles + ntiles * kTileCap) * 4 + 255) / 256 * 256;
+  a.wsum = base + off;
+  const bool fp64 = lat->storage == LBM_STORAGE_FP64;
+  const long long nchunks = (a.g.n + 31) >> 5;
+  if (fp64)
+    k_spread_clear<double><<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, (double *)field, chunks);
+  else
+    k_spread_clear<float><<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, field, chunks);
+  LBM_LAUNCH_CHECK("ibm_spread_tiled");
+  if (pt->n_markers == 0) return LBM_OK;
+  const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
+  if (fp64) {
+    k_spread_bin<double><<<nb, kIbmThreads, 0, s>>>(a);
+    if (mode == 0)
+      k_spread_tile<double, 0><<<(unsigned)ntiles, kTileNodes, 0, s>>>(a);
+    else
+      k_spread_tile<double, 1><<<(unsigned)ntiles, kTileNodes, 0, s>>>(a);
+  } else {
+    k_spread_bin<float><<<nb, kIbmThreads, 0, s>>>(a);
+    if (mode == 0)
+      k_spread_tile<float, 0><<<(unsigned)ntiles, kTileNodes, 0, s>>>(a);
+    else
+      k_spread_tile<float, 1><<<(unsigned)ntiles, kTileNodes, 0, s>>>(a);
+  }
+  LBM_LAUNCH_CHECK("ibm_spread_tiled");
   return LBM_OK;
 }
 

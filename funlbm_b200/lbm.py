@@ -414,7 +414,10 @@ class LBMD3(LBMBase):
         self._fol = [torch.zeros(n * 3, device=dev, dtype=rdt) for _ in range(2)]
         nch = (n + 31) // 32
         self._chunks = [torch.zeros(nch, dtype=torch.uint8, device=dev) for _ in range(2)]
-        self._owner = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        # scratch of the tiled spreading (tile lists, weight sums), zeroed once
+        nm = int(self.particle_swarm.struct().n_markers) if self.particle_swarm.particles else 0
+        nb = _lib.load().ibm_spread_tiled_scratch_bytes(ctypes_ref(self.flow.lattice.desc), nm)
+        self._spread_scratch = torch.zeros(nb, dtype=torch.uint8, device=dev)
         self._fi = 0          # index of the buffer the next spread writes
         self._status_ibm = torch.zeros(1, dtype=torch.int32, device=dev)
         # FOL of the state being entered (zero after init): the next step's
@@ -470,8 +473,8 @@ class LBMD3(LBMBase):
                  int(self.step), ptr(self._status_ibm), s)
         mode = 0 if self.config.ibm_mode == "reference" else 1
         sw_struct = self.particle_swarm.struct() if parts else _empty_particles()
-        call("ibm_spread", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode, ptr(F_new),
-             ptr(C_new), ptr(self._owner), s)
+        call("ibm_spread_tiled", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode, ptr(F_new),
+             ptr(C_new), ptr(self._spread_scratch), self._spread_scratch.numel(), s)
         if parts:
             # update_from_lar and Particle.update (with the next step's wall
             # markers) in one launch: nothing after spreading reads the old

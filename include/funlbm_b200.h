@@ -272,6 +272,18 @@ int rigid_wall_and_update(const lbm_lattice *lat, const lbm_particles *pt, int32
 int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
                uint8_t *chunks, int32_t *owner, void *stream);
 
+/* LBMD3.lagrange_to_flow (lbm/lbm3d.py:102-119) as ibm_spread, resolved in
+ * 8 x 8 x 8-node tiles in shared memory: one pass lists each marker under the
+ * tiles its stencil touches; one block per tile then takes the last writer of
+ * every node (mode 0) or sums the contributions (mode 1) in shared memory and
+ * writes each node once.  Mode 0 gives ibm_spread's field bit for bit.
+ * `scratch`: caller-owned device memory of at least
+ * ibm_spread_tiled_scratch_bytes(lat, pt->n_markers) bytes, zero before its
+ * first use (every call leaves the part that must start at zero at zero). */
+size_t ibm_spread_tiled_scratch_bytes(const lbm_lattice *lat, int32_t n_markers);
+int ibm_spread_tiled(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, float *field,
+                     uint8_t *chunks, void *scratch, size_t scratch_bytes, void *stream);
+
 /* Allocation-free ibm_spread.  No counterpart in the reference.  For callers
  * that cannot allocate device memory themselves -- a host program that only
  * has the lattice's own buffers (a solver coupled in through this C ABI from

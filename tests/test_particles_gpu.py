@@ -274,3 +274,61 @@ def LBMD3_with(parts, storage):
     init_with(lbm, None)
     run(lbm, 3)
     return lbm
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp64"])
+def test_tiled_spreading_matches_ibm_spread(storage):
+    """ibm_spread_tiled (shared-memory tiles) against ibm_spread (global
+    claims): the same field bit for bit in reference mode (last writer wins)
+    and within 1e-5 of its maximum in accumulate mode (summation order), the
+    same chunk flags, on two calls in a row; including a tile whose marker
+    list overflows (a dozen coincident spheres: the tile scans every marker)
+    and a body against the lattice's last nodes."""
+    import ctypes
+
+    from funlbm_b200 import _lib
+    from funlbm_b200._lib import ptr
+    from funlbm_b200.lattice import Lattice, tau_float32
+    from funlbm_b200.particle import ParticleConfig, ParticleSwarm
+
+    dt = torch.float64 if storage == "fp64" else torch.float32
+    shape = (30, 26, 28)
+    lat = Lattice(19, shape, [1200] * 6, tau_float32(0.1), storage=storage, device="cuda",
+                  allocate=False)
+    bodies = [(3, [8.0, 9.5, 10.2]), (2.5, [11.3, 12.0, 12.7]), (4, [24.6, 20.4, 22.1])]
+    bodies += [(3, [17.2, 6.3, 8.8])] * 12             # one tile sees > 512 markers
+    cfgs = [ParticleConfig().from_json({"type": "sphere", "r": r, "coord": {"center": c}})
+            for r, c in bodies]
+    sw = ParticleSwarm(cfgs, device="cuda", dtype=dt)
+    sw.init()
+    sw.update()
+    n = lat.n
+    nch = (n + 31) // 32
+    lib = _lib.load()
+    nbytes = lib.ibm_spread_tiled_scratch_bytes(ctypes.byref(lat.desc), sw.struct().n_markers)
+    scratch = torch.zeros(nbytes, dtype=torch.uint8, device="cuda")
+    for mode in (0, 1):
+        fa = torch.zeros(3 * n, device="cuda", dtype=dt)
+        fb = torch.zeros(3 * n, device="cuda", dtype=dt)
+        ca = torch.zeros(nch, dtype=torch.uint8, device="cuda")
+        cb = torch.zeros(nch, dtype=torch.uint8, device="cuda")
+        owner = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        for call in range(2):
+            if call:
+                sw.cx.add_(torch.tensor([0.37, -0.21, 0.44], device="cuda", dtype=dt))
+                sw.update()
+            g = torch.Generator(device="cpu").manual_seed(10 + call)
+            sw.lF.copy_((0.01 * torch.randn(sw.lF.shape, generator=g)).to(dt))
+            st = ctypes.byref(sw.struct())
+            _lib.call("ibm_spread", ctypes.byref(lat.desc), st, mode, ptr(fa), ptr(ca), ptr(owner),
+                      lat.stream())
+            _lib.call("ibm_spread_tiled", ctypes.byref(lat.desc), st, mode, ptr(fb), ptr(cb),
+                      ptr(scratch), nbytes, lat.stream())
+            torch.cuda.synchronize()
+            a, b = fa.cpu().numpy(), fb.cpu().numpy()
+            assert np.abs(a).max() > 0
+            if mode == 0:
+                assert np.array_equal(a, b), (call, np.abs(a - b).max())
+            else:
+                assert np.abs(a - b).max() <= 1e-5 * np.abs(a).max(), call
+            assert np.array_equal(ca.cpu().numpy(), cb.cpu().numpy()), (mode, call)
