@@ -10,7 +10,10 @@ import os
 import threading
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "liblbm_b200.so")
+# FUNLBM_B200_CHECKED=1 selects the bounds-checked build (python -m
+# funlbm_b200.build --checked): same results, index checks in every kernel
+LIB_PATH = os.path.join(PKG, "liblbm_b200_checked.so" if os.environ.get("FUNLBM_B200_CHECKED") == "1"
+                        else "liblbm_b200.so")
 
 LBM_OK = 0
 LBM_ERR_INVALID = 1
@@ -125,6 +128,7 @@ SIGNATURES = {
     "ibm_spread_tiled": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),
     "rigid_extremes": (I, [_PART, _P]),
     "lbm_debug_set_wait_limit": (None, [ctypes.c_int64]),
+    "lbm_debug_bounds_faults": (ctypes.c_int64, [ctypes.c_int32]),
     "lbm_last_error": (ctypes.c_char_p, []),
     "lbm_version": (ctypes.c_char_p, []),
 }

@@ -27,6 +27,28 @@ constexpr unsigned kTmaWaitPollsDefault = 1u << 24;
 // poll limit of its consumer waits for the next launches (lbm_debug_set_wait_limit)
 unsigned tma_wait_polls();
 
+// Bounds-checked build: every translation unit registers a reader of its own
+// violation counter (g_lbm_oob) with the library (lbm_debug_bounds_faults).
+using OobReader = unsigned long long (*)(bool reset);
+void register_oob_reader(OobReader r);
+#ifdef LBM_BOUNDS_CHECK
+namespace {
+unsigned long long read_oob(bool reset) {
+  unsigned long long v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_lbm_oob, sizeof(v)) != cudaSuccess) return ~0ull;
+  if (reset) {
+    const unsigned long long z = 0;
+    cudaMemcpyToSymbol(g_lbm_oob, &z, sizeof(z));
+  }
+  return v;
+}
+struct OobRegistration {
+  OobRegistration() { register_oob_reader(read_oob); }
+};
+const OobRegistration oob_registration;
+}  // namespace
+#endif
+
 // Launch-error check after a kernel launch.
 #define LBM_LAUNCH_CHECK(where)                              \
   do {                                                       \

@@ -1,6 +1,8 @@
 // Error reporting, lattice validation and Geom construction for the C ABI.
 #include <atomic>
 #include <cmath>
+#include <mutex>
+#include <vector>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -15,6 +17,19 @@ std::atomic<unsigned> g_tma_wait_polls{kTmaWaitPollsDefault};
 }
 
 unsigned tma_wait_polls() { return g_tma_wait_polls.load(std::memory_order_relaxed); }
+
+namespace {
+std::mutex g_oob_mu;
+std::vector<OobReader> &oob_readers() {
+  static std::vector<OobReader> v;
+  return v;
+}
+}  // namespace
+
+void register_oob_reader(OobReader r) {
+  std::lock_guard<std::mutex> lock(g_oob_mu);
+  oob_readers().push_back(r);
+}
 
 void set_error(const char *fmt, ...) {
   va_list ap;
@@ -182,6 +197,22 @@ size_t lbm_face_plane_floats(const lbm_lattice *lat) {
 }
 
 int lbm_lattice_check(const lbm_lattice *lat) { return lbm::check_lattice(lat); }
+
+int64_t lbm_debug_bounds_faults(int32_t reset) {
+#ifdef LBM_BOUNDS_CHECK
+  std::lock_guard<std::mutex> lock(lbm::g_oob_mu);
+  unsigned long long total = 0;
+  for (auto r : lbm::oob_readers()) {
+    const unsigned long long v = r(reset != 0);
+    if (v == ~0ull) return -2;
+    total += v;
+  }
+  return (int64_t)total;
+#else
+  (void)reset;
+  return -1;
+#endif
+}
 
 void lbm_debug_set_wait_limit(int64_t polls) {
   const unsigned v = polls < 0 ? lbm::kTmaWaitPollsDefault

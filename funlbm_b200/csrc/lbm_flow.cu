@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(kThreads)
   if (face && face_rho_ != nullptr) write_face_rho<Q>(g, static_cast<R *>(face_rho_), x, y, z, rho);
   typename St::T *fa = static_cast<typename St::T *>(fa_);
   const long long pidx = ((long long)x * g.ny + y) * g.pz + z;
+  if (!lbm_in(pidx < g.np)) return;
 #pragma unroll
   for (int i = 0; i < Q; ++i) St::store(fa + (long long)i * g.np + pidx, f[i], V::template wr<R>(i));
 }

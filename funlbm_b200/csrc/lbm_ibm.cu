@@ -185,6 +185,11 @@ __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
     int x, y, z;
     R w;
     if (stencil_slot(a.g, l, slot, x, y, z, w)) {
+      if (!lbm_in(x >= 0 && x < a.g.nx && y >= 0 && y < a.g.ny && z >= 0 && z < a.g.nz)) {
+        x = 0;
+        y = 0;
+        z = 0;
+      }
       const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
       R rho, ux, uy, uz;
       if (a.fa != nullptr) {
@@ -447,6 +452,7 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
     in_box = stencil_slot(a.g, l, slot, x, y, z, w);
   }
   const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
+  if (in_box && !lbm_in(idx >= 0 && idx < a.g.n)) in_box = false;
   if (PASS == 0 || PASS == 2) {
     if (!in_box) return;
     if (PASS == 0) {
@@ -528,6 +534,7 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread_bin(const TileArgs a) {
     for (int j = lo[1] / kTile; j <= (hi[1] - 1) / kTile; ++j)
       for (int k = lo[2] / kTile; k <= (hi[2] - 1) / kTile; ++k) {
         const int t = (i * a.ty + j) * a.tz + k;
+        if (!lbm_in(t >= 0 && t < a.tx * a.ty * a.tz)) continue;
         const int pos = atomicAdd(a.tile_count + t, 1);
         if (pos < kTileCap) a.tile_list[(long long)t * kTileCap + pos] = m;
       }
@@ -578,7 +585,7 @@ __global__ void __launch_bounds__(kTileNodes) k_spread_tile(const TileArgs a) {
   __syncthreads();
   const int x = ox + tid / (kTile * kTile), y = oy + (tid / kTile) % kTile, z = oz + tid % kTile;
   const int m = s_owner[tid];
-  if (m >= 0 && x < a.g.nx && y < a.g.ny && z < a.g.nz) {
+  if (m >= 0 && lbm_in(x < a.g.nx && y < a.g.ny && z < a.g.nz)) {
     const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
     a.chunks[idx >> 5] = 1;
     if constexpr (MODE == 0) {

@@ -14,6 +14,23 @@
 
 namespace lbm {
 
+// Bounds-checked build (-DLBM_BOUNDS_CHECK): kernels verify their index
+// invariants before each access (node inside the lattice, population index
+// inside the pitched buffer, pull source inside the lattice, field index
+// inside the field); a violation is counted in this translation unit's
+// g_lbm_oob and the access is skipped or clamped to a valid index
+// (lbm_debug_bounds_faults reads the counts).  Without the flag lbm_in is
+// always true and the checks compile away.
+#ifdef LBM_BOUNDS_CHECK
+static __device__ unsigned long long g_lbm_oob;
+__device__ __forceinline__ bool lbm_in(bool ok) {
+  if (!ok) atomicAdd(&g_lbm_oob, 1ull);
+  return ok;
+}
+#else
+__device__ __forceinline__ constexpr bool lbm_in(bool) { return true; }
+#endif
+
 // Compile-time loop: calls fn(std::integral_constant<int, I>) for I < N, so
 // every population index is a constant and f[Q] stays in registers.
 template <typename F, int... I>
@@ -360,6 +377,11 @@ __device__ __forceinline__ typename Storage<S>::R pull_one(
         corr = R(2) * (rho_t * V::template wr<R>(I)) * eu * Cst<R>::inv_cs2(g);
       }
     }
+  }
+  if (!lbm_in(sx >= 0 && sx < g.nx && sy >= 0 && sy < g.ny && sz >= 0 && sz < g.nz)) {
+    sx = 0;
+    sy = 0;
+    sz = 0;
   }
   const long long src = ((long long)sx * g.ny + sy) * g.pz + sz;
   const R w_sd = sd == I ? V::template wr<R>(I) : V::template wr<R>(V::rev(I));

@@ -169,6 +169,7 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   const ChunkForce cf = chunk_force<FORCE>(a, idx);
   a.dec(idx, x, y, z);
   const unsigned pidx = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.pz + (unsigned)z;
+  if (!lbm_in(x < a.g.nx && y < a.g.ny && z < a.g.nz && pidx < (unsigned)a.g.np)) return;
   using R = typename St::R;
   const R *face_rho = static_cast<const R *>(a.face_rho_in);
   const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
@@ -256,6 +257,7 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const StepArgs a,
     a.dec(idx, x, y, z);
     const bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
     const unsigned pidx = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.pz + (unsigned)z;
+    if (!lbm_in(x < a.g.nx && y < a.g.ny && z < a.g.nz && pidx < (unsigned)a.g.np)) continue;
     R f[Q];
     if (row_in)
       pull_row_node<Q, S, true>(a.p, a.g, face_rho, pidx, x, y, z, f);
@@ -371,6 +373,8 @@ __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0,
   unsigned bad = 0;
 #pragma unroll 1
   for (int k = 0; k < count; ++k) {
+    if (!lbm_in(z0 + k < a.g.nz && pidx0 + k < (unsigned)a.g.np && idx0 + k < (unsigned)a.g.n))
+      continue;
     R f[Q];
     pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, face_rho, f);
     // the nodes may lie in two chunks
@@ -413,6 +417,9 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
     face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, a.g.nz - z0, x, y, z0);
     return;
   }
+  if (!lbm_in(x < a.g.nx && y < a.g.ny && pidx0 + NZ <= (unsigned)a.g.np &&
+              idx0 + NZ <= (unsigned)a.g.n))
+    return;
   constexpr bool kCompact = COMPACT;
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {
@@ -523,6 +530,9 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
     face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, a.g.nz - z0, x, y, z0);
     return;
   }
+  if (!lbm_in(x < a.g.nx && y < a.g.ny && pidx0 + NZ <= (unsigned)a.g.np &&
+              idx0 + NZ <= (unsigned)a.g.n))
+    return;
   constexpr bool kCompact = COMPACT;
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {

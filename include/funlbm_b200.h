@@ -344,6 +344,13 @@ int rigid_update_markers(const lbm_particles *pt, void *stream);
  * without a fault.  Populations of a step that timed out are incomplete. */
 void lbm_debug_set_wait_limit(int64_t polls);
 
+/* Bounds-checked builds (liblbm_b200_checked.so, compiled with
+ * -DLBM_BOUNDS_CHECK; no counterpart in the reference): the number of index
+ * violations the kernels caught since the last reset (each one skipped or
+ * clamped its access), over all translation units; reset != 0 zeroes the
+ * counts.  -1 in a normal build, -2 if a count could not be read. */
+int64_t lbm_debug_bounds_faults(int32_t reset);
+
 /* Thread-local message of the last failed call. */
 const char *lbm_last_error(void);
 

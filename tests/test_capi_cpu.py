@@ -132,3 +132,9 @@ def test_gpu_required_without_cuda():
 
     with pytest.raises(RuntimeError):
         LBMD3(config=Config().from_json({"flow": {"size": [4, 4, 4]}}))
+
+
+def test_normal_build_has_no_bounds_counters(lib):
+    """Only the bounds-checked build (FUNLBM_B200_CHECKED=1) counts index
+    violations; the normal library says so with -1."""
+    assert lib.lbm_debug_bounds_faults(0) == -1
