@@ -80,7 +80,8 @@ def tune(lat, force=None, iters=6, warmup=2, verbose=False):
     per_x = 2 * lat.q * ny * nz * BYTES[lat.storage]
     px = max(4, min(nx, PROXY_BYTES // max(per_x, 1)))
     proxy = Lattice(lat.q, (px, ny, nz), lat.faces, lat.tau, storage=lat.storage,
-                    face_uw=lat.face_uw, re_mu=lat.re_mu, device=lat.device)
+                    face_uw=lat.face_uw, re_mu=lat.re_mu, device=lat.device,
+                    pitch=lat.pz != nz)      # the lattice's own row layout
     proxy.init(None)
     timings = {}
     start = torch.cuda.Event(enable_timing=True)
