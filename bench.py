@@ -516,7 +516,8 @@ def cpu_baseline(args, seconds=12.0):
 # served stream (continuous batching) vs the same requests one by one
 # ---------------------------------------------------------------------------
 def make_requests(n, seed=0, steps=(500, 5000)):
-    """Seeded mixed stream: node counts per axis uniform in {32, 48, ..., 192},
+    """Seeded mixed stream: grid size per axis uniform in {32, 48, ..., 192}
+    (the reference's size, so size + 1 nodes: rows of odd length),
     D3Q19 / D3Q27 50/50, fp32 / fp16s 50/50, random WALL / PERIODICAL faces,
     0-8 spheres or ellipsoids of radius 4-8, steps uniform in `steps`."""
     from funlbm_b200.serve import Request
@@ -544,7 +545,7 @@ def make_requests(n, seed=0, steps=(500, 5000)):
                               "rou": 1.2, "coord": {"center": center, "alpha": float(rot[0]),
                                                     "beta": float(rot[1]), "gamma": float(rot[2])}})
         cfg = {"device": "cuda", "log_per_steps": 10 ** 9, "file": {"per_steps": 10 ** 9},
-               "flow": {"size": [d - 1 for d in dims], "param_type": "D3Q%d" % q,
+               "flow": {"size": list(dims), "param_type": "D3Q%d" % q,
                         "param": {"mu": 0.05, "gl": 1e-5}, "precision": {"storage": storage},
                         "boundary": {k: {"code": str(rng.choice(["WALL", "PERIODICAL"]))}
                                      for k in faces}},
