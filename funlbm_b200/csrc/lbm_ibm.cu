@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
   const int pi = blockIdx.x;
   const int m0 = P.offset[pi], m1 = P.offset[pi + 1];
   __shared__ double s_sum[3][kRigidThreads / 32];
-  __shared__ R s_cx[3], s_cw[3];
+  __shared__ R s_cx[3], s_ang[3];
   __shared__ R s_v[6][kRigidThreads / 32];
   __shared__ int s_i[6][kRigidThreads / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -806,17 +806,20 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
       P.cT[3 * pi + k] = ct;
       const R cw = P.cw[3 * pi + k] + R(0.1) * ct * (R)a.dt / P.inertia[3 * pi + k];
       P.cw[3 * pi + k] = cw;
-      s_cw[k] = cw;
+      // angle += cw (particle/coord.py:107), shared so that no thread reads
+      // the rotation vector after it is overwritten
+      const R ang = P.angle[3 * pi + k] + cw;
+      s_ang[k] = ang;
+      P.angle[3 * pi + k] = ang;
     }
   }
-  __syncthreads();   // every thread has read lx for the torque; cw is final
+  __syncthreads();   // every thread has read lx for the torque; cw and angle are final
 
-  // -- angle += cw; lx = R(angle) X0 + cx   (particle/coord.py:87-108)
+  // -- lx = R(angle) X0 + cx   (particle/coord.py:87-108)
   double v[3];
-  R ang[3], c[3];
+  R c[3];
   for (int k = 0; k < 3; ++k) {
-    ang[k] = P.angle[3 * pi + k] + s_cw[k];
-    v[k] = ang[k];
+    v[k] = s_ang[k];
     c[k] = s_cx[k];
   }
   const double th = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
@@ -843,8 +846,6 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
       P.lx[3 * m + k] = (R)r + c[k];
     }
   }
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 3; ++k) P.angle[3 * pi + k] = ang[k];
   if (a.p.extreme == nullptr) return;
   __syncthreads();   // the new positions are written
   int ext[6];
