@@ -269,8 +269,10 @@ class FlowD3(Flow):
         X, Y, Z = self.shape
         e = torch.tensor(VELOCITY_SETS[self.q][0], dtype=torch.float64, device=self.device)
         rou = self._f.sum(0).view(X, Y, Z, 1)
-        u = (e.t() @ self._f).t().reshape(X, Y, Z, 3)
-        u = (u + self._FOL / 2) / rou
+        # (a reshape of the transposed product is a strided view: make the
+        # [x][y][z][3] layout the kernels write explicit)
+        u = (e.t() @ self._f).t().contiguous().view(X, Y, Z, 3)
+        u = ((u + self._FOL / 2) / rou).contiguous()
         for a in range(3):
             for pl in (0, -1):
                 idx = [slice(None)] * 3
@@ -295,6 +297,11 @@ class FlowD3(Flow):
         force, fields = self._last_force
         if self._f is None:        # released while stepping in the fused form
             self._f = torch.empty((self.q, self.n), device=self.device, dtype=lat.real_dtype)
+        # the kernel writes dense [x][y][z](3) arrays through the raw pointers
+        if not self._rou.is_contiguous():
+            self._rou = self._rou.contiguous()
+        if not self._u.is_contiguous():
+            self._u = self._u.contiguous()
         lat.observe(force, f=self._f, rho=self._rou, u=self._u)
         self._p = self._rou / 3.0
         new_field, new_uniform = fields
