@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--vs-fp64", action="store_true",
                     help="with --case: run the case in fp64, fp32, fp16s and bf16s storage and "
                          "report each one's error against the fp64 run")
+    ap.add_argument("--spread", default=None, choices=["claims", "tiles"],
+                    help="with --case: the spreading kernels (ibm.spread)")
     ap.add_argument("--case-steps", type=int, default=None,
                     help="steps of the --vs-fp64 runs (default: the case's stated horizon)")
     ap.add_argument("--ke-errors", action="store_true",
@@ -690,6 +692,8 @@ def run_case_sphere(args):
         cfg, label = ellipsoids_config(args.storage), "D3Q27 %s multi-ellipsoid 257x129x129"
     else:
         cfg, label = sphere_config(args.storage), "D3Q19 %s sphere free-fall 161x65x65"
+    if args.spread:
+        cfg["ibm"] = {"spread": args.spread}
     lbm = LBMD3(config=Config().from_json(cfg))
     lbm.init()
     for _ in range(args.warmup):

@@ -20,6 +20,8 @@ reference, which logs every step), ``graph_steps`` (``run`` replays the
 fused steps between logging / checkpoint steps from captured CUDA graphs of
 up to this many steps; default 32, 0 = never), ``ibm.mode`` (``reference`` = the
 reference's last-writer-wins spreading, ``accumulate`` = summed spreading),
+``ibm.spread`` (``claims`` = global per-node claims, the default; ``tiles`` =
+8^3 tiles resolved in shared memory; the same field),
 ``flow.precision.storage``, ``flow.body_force``, ``flow.init_field``,
 ``log.db`` (a SQLite file for the per-step records the reference keeps in
 its key-value store; default none).  Logging at the cadence runs off the
@@ -65,6 +67,7 @@ class Config(BaseConfig):
         self.ibm_mode = "reference"
         self.graph_steps = 32
         self.log_db = None
+        self.ibm_spread = "claims"
 
     def _from_json(self, config_json: dict, *args, **kwargs) -> "Config":
         self.dt = deep_get(config_json, "dt") or self.dt
@@ -85,6 +88,9 @@ class Config(BaseConfig):
         gs = deep_get(config_json, "graph_steps")
         self.graph_steps = self.graph_steps if gs is None else int(gs)
         self.log_db = deep_get(config_json, "log.db") or self.log_db
+        self.ibm_spread = deep_get(config_json, "ibm.spread") or self.ibm_spread
+        if self.ibm_spread not in ("claims", "tiles"):
+            raise ValueError("ibm.spread must be 'claims' or 'tiles'")
         self.ibm_mode = deep_get(config_json, "ibm.mode") or self.ibm_mode
         if self.ibm_mode not in ("reference", "accumulate"):
             raise ValueError("ibm.mode must be 'reference' or 'accumulate'")
@@ -414,10 +420,14 @@ class LBMD3(LBMBase):
         self._fol = [torch.zeros(n * 3, device=dev, dtype=rdt) for _ in range(2)]
         nch = (n + 31) // 32
         self._chunks = [torch.zeros(nch, dtype=torch.uint8, device=dev) for _ in range(2)]
-        # scratch of the tiled spreading (tile lists, weight sums), zeroed once
-        nm = int(self.particle_swarm.struct().n_markers) if self.particle_swarm.particles else 0
-        nb = _lib.load().ibm_spread_tiled_scratch_bytes(ctypes_ref(self.flow.lattice.desc), nm)
-        self._spread_scratch = torch.zeros(nb, dtype=torch.uint8, device=dev)
+        if self.config.ibm_spread == "tiles":
+            # scratch of the tiled spreading (tile lists, weight sums), zeroed once
+            nm = int(self.particle_swarm.struct().n_markers) if self.particle_swarm.particles else 0
+            nb = _lib.load().ibm_spread_tiled_scratch_bytes(ctypes_ref(self.flow.lattice.desc), nm)
+            self._spread_scratch = torch.zeros(nb, dtype=torch.uint8, device=dev)
+        else:
+            # claim array of the global-claim spreading, -1 between calls
+            self._owner = torch.full((n,), -1, dtype=torch.int32, device=dev)
         self._fi = 0          # index of the buffer the next spread writes
         self._status_ibm = torch.zeros(1, dtype=torch.int32, device=dev)
         # FOL of the state being entered (zero after init): the next step's
@@ -473,8 +483,13 @@ class LBMD3(LBMBase):
                  int(self.step), ptr(self._status_ibm), s)
         mode = 0 if self.config.ibm_mode == "reference" else 1
         sw_struct = self.particle_swarm.struct() if parts else _empty_particles()
-        call("ibm_spread_tiled", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode, ptr(F_new),
-             ptr(C_new), ptr(self._spread_scratch), self._spread_scratch.numel(), s)
+        if self.config.ibm_spread == "tiles":
+            call("ibm_spread_tiled", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode,
+                 ptr(F_new), ptr(C_new), ptr(self._spread_scratch), self._spread_scratch.numel(),
+                 s)
+        else:
+            call("ibm_spread", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode, ptr(F_new),
+                 ptr(C_new), ptr(self._owner), s)
         if parts:
             # update_from_lar and Particle.update (with the next step's wall
             # markers) in one launch: nothing after spreading reads the old
