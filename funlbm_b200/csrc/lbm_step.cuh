@@ -199,7 +199,7 @@ constexpr int scalar_min_blocks() {
 }
 
 template <int Q, int S, bool FORCE>
-__global__ void __launch_bounds__(kThreads, (scalar_min_blocks<Q, S>())) k_step(const StepArgs a) {
+__global__ void __launch_bounds__(kThreads, (scalar_min_blocks<Q, S>())) k_step(const __grid_constant__ StepArgs a) {
   step_scalar_body<Q, S, FORCE>(a, blockIdx.x * kThreads + threadIdx.x);
 }
 
@@ -235,7 +235,7 @@ __device__ __forceinline__ void stat_add(StatAcc &s, int k, double v) {
 }
 
 template <int Q, int S, bool FORCE>
-__global__ void __launch_bounds__(kStatsThreads) k_stats(const StepArgs a,
+__global__ void __launch_bounds__(kStatsThreads) k_stats(const __grid_constant__ StepArgs a,
                                                          unsigned long long *out) {
   using St = Storage<S>;
   using T = typename St::T;
@@ -359,12 +359,15 @@ __host__ __device__ constexpr bool compact_face_rows() {
 
 // Nodes of a row on an x / y face (under 1 % of a large lattice), or the
 // last nodes of a row whose length is not a multiple of a thread's NZ: one at
-// a time through the general face rules, in a loop that is not unrolled, so a
-// vector kernel carries one copy of this code instead of NZ.  Same per-node
-// arithmetic.  idx0 / pidx0: dense / population index of node (x, y, z0).
+// a time through the general face rules, in a loop that is not unrolled and
+// a function that is not inlined, so a vector kernel carries one copy of this
+// code however many places call it (it is reached from two).  The kernels
+// take their StepArgs as __grid_constant__ parameters, so the reference it
+// receives points at the parameter itself (no per-thread copy).  Same
+// per-node arithmetic.  idx0 / pidx0: dense / population index of node (x, y, z0).
 template <int Q, int S, bool FORCE>
-__device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, unsigned pidx0,
-                                               int count, int x, int y, int z0) {
+__device__ __noinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, unsigned pidx0,
+                                            int count, int x, int y, int z0) {
   using St = Storage<S>;
   using T = typename St::T;
   using R = typename St::R;
@@ -642,7 +645,7 @@ constexpr int vec_min_blocks() {
 }
 
 template <int Q, int S, bool FORCE, int NZ, int TB>
-__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>())) k_step_vec(const StepArgs a) {
+__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>())) k_step_vec(const __grid_constant__ StepArgs a) {
   step_vec_body<Q, S, FORCE, NZ>(a, blockIdx.x * TB + threadIdx.x);
 }
 
@@ -654,7 +657,7 @@ __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>())) k
 // D3Q27, so it is a tuner candidate, not a default.
 template <int Q, int S, bool FORCE, int TB>
 __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, 2, TB, FORCE>()))
-    k_step_odd(const StepArgs a, const FastDiv per_row, unsigned rows) {
+    k_step_odd(const __grid_constant__ StepArgs a, const FastDiv per_row, unsigned rows) {
   const unsigned t = blockIdx.x * TB + threadIdx.x;
   const unsigned row = fdiv(t, per_row);
   if (row >= rows) return;
@@ -762,7 +765,7 @@ __device__ __forceinline__ float2 sm_pair(const typename Storage<S>::T *p) {
 }
 
 template <int Q, int S, bool FORCE>
-__global__ void __launch_bounds__(kTmaThreads) k_step_tma(const StepArgs a, const TmaPlan p) {
+__global__ void __launch_bounds__(kTmaThreads) k_step_tma(const __grid_constant__ StepArgs a, const TmaPlan p) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
