@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kThreads) k_stream(const Geom g, const NodeDec
       } else if (code == LBM_BC_NON_EQUILIBRIUM) {
         const int nbx = fc == 0 ? 1 : g.nx - 2;
         const long long nb = ((long long)nbx * g.ny + y) * g.nz + z;
-        const float rolled = pull_rolled<Q, LBM_STORAGE_FP32>(fin, g, i, nbx, y, z);
+        const float rolled = pull_rolled<Q>(fin, g, i, nbx, y, z);
         v = feq[(long long)i * g.n + idx] + (rolled - feq[(long long)i * g.n + nb]);
       } else {
         v = fin[(long long)V::rev(i) * g.n + idx];

@@ -133,22 +133,34 @@ template <int S>
 struct Storage;
 
 // The fused step works on the stored quantity itself (its "working value"):
-// f for FP32, the deviation d = f - w_i for the shifted forms (kDev), whose
-// moments and collision are restated for d (dev_moments / collide_dev), so
-// no weight is added on load or subtracted on store.  work / put / work2 /
-// put2 move working values; load / store always give f.
+// the deviation d = f - w_i for the shifted forms (kDev: FP32 and both 16-bit
+// storages), whose moments and collision are restated for d (dev_moments /
+// collide_dev), so no weight is added on load or subtracted on store; f
+// itself for FP64.  work / put / work2 / put2 move working values; load /
+// store always give f.
+//
+// FP32 stores the deviation too.  At the low Mach numbers of the reference's
+// cases a population f ~ w_i ~ 0.05 carries its velocity part (w rho e.u /
+// cs^2 ~ 1e-6) in its last ten bits, and a body or IBM force adds ~17 units
+// in the last place per step: stored as f, those increments round with the
+// same bias every step of a nearly steady flow, and the float32 run drifts
+// from the float64 one (measured on B200: twice the reference's own float32
+// drift on the 33 x 33 x 65 Poiseuille channel after 2000 steps, ten times
+// in the sedimenting sphere's velocity after 5000).  Stored as d ~ 1e-6 the
+// same 32 bits resolve the signal to ~1e-7 of itself, at the same bytes per
+// node.
 template <>
 struct Storage<LBM_STORAGE_FP32> {
   using T = float;
   using R = float;   // arithmetic type of the kernels
   static constexpr int kBits = 32;
-  static constexpr bool kDev = false;
+  static constexpr bool kDev = true;
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
   __device__ __forceinline__ static float cvt(T v) { return v; }
   __device__ __forceinline__ static float work(const T *p) { return __ldg(p); }
   __device__ __forceinline__ static void put(T *p, float v) { *p = v; }
-  __device__ __forceinline__ static float load(const T *p, float) { return __ldg(p); }
-  __device__ __forceinline__ static void store(T *p, float v, float) { *p = v; }
+  __device__ __forceinline__ static float load(const T *p, float w) { return w + __ldg(p); }
+  __device__ __forceinline__ static void store(T *p, float v, float w) { *p = v - w; }
 };
 template <>
 struct Storage<LBM_STORAGE_FP16S> {
@@ -490,16 +502,16 @@ __device__ __forceinline__ void pull_row_node(const StepPlanes &p, const Geom &g
 // Rolled value (periodic wrap on every axis, no face rule): what the
 // reference's f holds at a node before the face overrides run.  Used by the
 // NON_EQUILIBRIUM faces, which read plane 1 / plane X-2 right after the roll.
-template <int Q, int S>
-__device__ __forceinline__ float pull_rolled(const typename Storage<S>::T *__restrict__ fa,
-                                             const Geom &g, int i, int x, int y, int z) {
+template <int Q>
+__device__ __forceinline__ float pull_rolled(const float *__restrict__ fa, const Geom &g, int i,
+                                             int x, int y, int z) {
   using V = VSet<Q>;
   int sx = x - V::ex(i), sy = y - V::ey(i), sz = z - V::ez(i);
   sx = sx < 0 ? sx + g.nx : (sx >= g.nx ? sx - g.nx : sx);
   sy = sy < 0 ? sy + g.ny : (sy >= g.ny ? sy - g.ny : sy);
   sz = sz < 0 ? sz + g.nz : (sz >= g.nz ? sz - g.nz : sz);
   const long long src = ((long long)sx * g.ny + sy) * g.nz + sz;   // dense arrays only
-  return Storage<S>::load(fa + (long long)i * g.n + src, V::w(i));
+  return fa[(long long)i * g.n + src];
 }
 
 // ---------------------------------------------------------------------------
@@ -665,7 +677,7 @@ __device__ __forceinline__ void dev_moments(const float d[Q], float fx, float fy
   });
   drho = r;
   rho = 1.f + r;
-  const float inv = __fdividef(1.f, rho);
+  const float inv = 1.f / rho;
   ux = face ? 0.f : LBM_FMA(0.5f, fx, jx) * inv;
   uy = face ? 0.f : LBM_FMA(0.5f, fy, jy) * inv;
   uz = face ? 0.f : LBM_FMA(0.5f, fz, jz) * inv;

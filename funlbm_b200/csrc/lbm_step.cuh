@@ -154,6 +154,44 @@ __device__ __forceinline__ void report_bad(unsigned *status, unsigned bad) {
   if (bad != 0 && status != nullptr) atomicOr(status, bad);
 }
 
+// Row padding of a pitched lattice (population index p, p + 1, ... up to the
+// row's pitch) is written by the kernel that writes the row's last node,
+// with any value: it is never a pull source and never observed, but a
+// 32-byte sector that a step writes only in part makes L2 fetch the rest
+// from DRAM before it can write the sector back (measured on B200 at 257^3
+// in FP32: +2 % DRAM reads and 16 % longer steps while the padding was left
+// unwritten).
+template <int Q, int S>
+__device__ __forceinline__ void put_row_padding(const StepArgs &a, unsigned p, int count,
+                                                const typename Storage<S>::R f[Q]) {
+  using St = Storage<S>;
+  using T = typename St::T;
+#pragma unroll 1
+  for (int j = 0; j < count; ++j) {
+    static_for<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      St::put(static_cast<T *>(a.p.dst[i]) + p + j, f[i]);
+    });
+  }
+}
+
+// A vector of padding only (a pitched row's last vector, past its nodes):
+// zero words, stored for the same reason.
+template <int Q, int S, int NZ>
+__device__ __forceinline__ void put_padding_vector(const StepArgs &a, unsigned pidx0) {
+  using St = Storage<S>;
+  using T = typename St::T;
+  constexpr int kWords = NZ * St::kBits / 32;
+  if (a.fb == nullptr) return;
+  Words<kWords> zero;
+#pragma unroll
+  for (int k = 0; k < kWords; ++k) zero.w[k] = 0u;
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    st_words(static_cast<T *>(a.p.dst[i]) + pidx0, zero);
+  });
+}
+
 // One node per thread, nodes in memory order so that each warp owns one
 // 32-node chunk.  Rows with interior (x, y) pull through pull_row_node;
 // rows on an x / y face take the general face rules.  FORCE adds cul_equ2
@@ -187,6 +225,8 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
       constexpr int i = decltype(ic)::value;
       St::put(static_cast<T *>(a.p.dst[i]) + pidx, f[i]);
     });
+    if (z == a.g.nz - 1 && a.g.pz > a.g.nz)
+      put_row_padding<Q, S>(a, pidx + 1, a.g.pz - a.g.nz, f);
   }
 }
 
@@ -358,16 +398,16 @@ __host__ __device__ constexpr bool compact_face_rows() {
 }
 
 // Nodes of a row on an x / y face (under 1 % of a large lattice), or the
-// last nodes of a row whose length is not a multiple of a thread's NZ: one at
-// a time through the general face rules, in a loop that is not unrolled and
-// a function that is not inlined, so a vector kernel carries one copy of this
+// last nodes of a pitched row under a WALL_WITH_SPEED top face: one at a
+// time through the general face rules, in a loop that is not unrolled and a
+// function that is not inlined, so a vector kernel carries one copy of this
 // code however many places call it (it is reached from two).  The kernels
 // take their StepArgs as __grid_constant__ parameters, so the reference it
 // receives points at the parameter itself (no per-thread copy).  Same
 // per-node arithmetic.  idx0 / pidx0: dense / population index of node (x, y, z0).
 template <int Q, int S, bool FORCE>
-__device__ __noinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, unsigned pidx0,
-                                            int count, int x, int y, int z0) {
+__device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, unsigned pidx0,
+                                            int count, int pad, int x, int y, int z0) {
   using St = Storage<S>;
   using T = typename St::T;
   using R = typename St::R;
@@ -388,6 +428,7 @@ __device__ __noinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, un
         constexpr int i = decltype(ic)::value;
         St::put(static_cast<T *>(a.p.dst[i]) + pidx0 + k, f[i]);
       });
+      if (k == count - 1 && pad > 0) put_row_padding<Q, S>(a, pidx0 + count, pad, f);
     }
   }
   report_bad(a.status, bad);
@@ -403,7 +444,7 @@ __device__ __noinline__ void face_row_nodes(const StepArgs &a, unsigned idx0, un
 // ALIGNED = false: the pair starts at any index (rows of odd length), so
 // its elements are loaded and stored one by one and its nodes may lie in two
 // different force chunks.
-template <int Q, int S, bool FORCE, int NZ, bool COMPACT, bool ALIGNED = true>
+template <int Q, int S, bool FORCE, int NZ, bool COMPACT, bool ALIGNED = true, bool PITCH = false>
 __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsigned pidx0) {
   using St = Storage<S>;
   using T = typename St::T;
@@ -414,25 +455,35 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
   if (pidx0 >= (unsigned)a.g.np) return;
   int x, y, z0;
   a.pdec(pidx0, x, y, z0);
-  if (z0 >= a.g.nz) return;                  // row padding
+  if constexpr (PITCH) {
+    if (z0 >= a.g.nz) {                      // row padding only
+      put_padding_vector<Q, S, NZ>(a, pidx0);
+      return;
+    }
+  }
   const unsigned idx0 = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.nz + (unsigned)z0;
-  if (z0 + NZ > a.g.nz) {                    // the last nodes of a row (pitched rows)
-    face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, a.g.nz - z0, x, y, z0);
+  // nodes inside the row (fewer than NZ in the last vector of a pitched row:
+  // the other lanes are padding, loaded and stored but not finished)
+  const int nv = PITCH && a.g.nz - z0 < NZ ? a.g.nz - z0 : NZ;
+  if (PITCH && nv < NZ && a.g.face[5] == LBM_BC_WALL_WITH_SPEED) {
+    face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, nv, NZ - nv, x, y, z0);
     return;
   }
   if (!lbm_in(x < a.g.nx && y < a.g.ny && pidx0 + NZ <= (unsigned)a.g.np &&
-              idx0 + NZ <= (unsigned)a.g.n))
+              idx0 + nv <= (unsigned)a.g.n))
     return;
   constexpr bool kCompact = COMPACT;
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {
     if (!row_in) {
-      face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, NZ, x, y, z0);
+      face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, nv, NZ - nv, x, y, z0);
       return;
     }
     row_in = true;
   }
-  const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
+  const bool bottom = z0 == 0, top = z0 + NZ >= a.g.nz;
+  // lane of the row's last node when it lies inside this vector (else NZ)
+  const int last = nv < NZ ? nv - 1 : NZ;
   Words<kWords> raw[Q];
   T extra[Q];
   if (row_in) {
@@ -447,7 +498,7 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
       if constexpr (ez > 0)
         extra[i] = St::raw(bottom ? static_cast<const T *>(a.p.zlo[i]) + pidx0 : ps - 1);
       if constexpr (ez < 0)
-        extra[i] = St::raw(top ? static_cast<const T *>(a.p.zhi[i]) + (pidx0 + NZ - 1) : ps + NZ);
+        extra[i] = St::raw(top ? static_cast<const T *>(a.p.zhi[i]) + (pidx0 + (nv - 1)) : ps + NZ);
     });
   }
   unsigned bad = 0;
@@ -467,9 +518,12 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
           f0[i] = pr == 0 ? St::cvt(extra[i]) : work2<S>(raw[i].w[pr > 0 ? pr - 1 : 0]).y;
           f1[i] = v.x;
         } else {
-          f0[i] = v.y;
-          f1[i] = pr == kWords - 1 ? St::cvt(extra[i])
-                                   : work2<S>(raw[i].w[pr < kWords - 1 ? pr + 1 : pr]).x;
+          // (the row's last node pulls the top face's value; a padding lane
+          // after it keeps any value: it is not finished)
+          f0[i] = 2 * pr == last ? St::cvt(extra[i]) : v.y;
+          f1[i] = pr == kWords - 1 || 2 * pr + 1 == last
+                      ? St::cvt(extra[i])
+                      : work2<S>(raw[i].w[pr < kWords - 1 ? pr + 1 : pr]).x;
         }
       });
       if (pr == 0 && bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
@@ -479,16 +533,19 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
     } else if constexpr (!kCompact) {
       const T *fa = static_cast<const T *>(a.fa);
       const float *face_rho = static_cast<const float *>(a.face_rho_in);
-      pull_general<Q, S, true>(fa, a.g, x, y, za, face_rho, f0);
-      pull_general<Q, S, true>(fa, a.g, x, y, za + 1, face_rho, f1);
+      // (padding lanes repeat the row's last node; they are not finished)
+      pull_general<Q, S, true>(fa, a.g, x, y, 2 * pr < nv ? za : a.g.nz - 1, face_rho, f0);
+      pull_general<Q, S, true>(fa, a.g, x, y, 2 * pr + 1 < nv ? za + 1 : a.g.nz - 1, face_rho, f1);
     }
     // (a pair may straddle two force chunks: dense rows of any length)
-    finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
-                                !row_in || za == 0 || za == a.g.nz - 1,
-                                chunk_force<FORCE>(a, idx0 + 2 * pr), bad);
-    finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
-                                !row_in || za + 1 == a.g.nz - 1,
-                                chunk_force<FORCE>(a, idx0 + 2 * pr + 1), bad);
+    if (2 * pr < nv)
+      finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
+                                  !row_in || za == 0 || za == a.g.nz - 1,
+                                  chunk_force<FORCE>(a, idx0 + 2 * pr), bad);
+    if (2 * pr + 1 < nv)
+      finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
+                                  !row_in || za + 1 == a.g.nz - 1,
+                                  chunk_force<FORCE>(a, idx0 + 2 * pr + 1), bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -506,19 +563,23 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
   report_bad(a.status, bad);
 }
 
-template <int Q, int S, bool FORCE, int NZ, bool COMPACT>
+template <int Q, int S, bool FORCE, int NZ, bool COMPACT, bool PITCH>
 __device__ __forceinline__ void step_vec_pairs(const StepArgs &a, const unsigned t) {
-  step_vec_pairs_at<Q, S, FORCE, NZ, COMPACT, true>(a, t * NZ);
+  step_vec_pairs_at<Q, S, FORCE, NZ, COMPACT, true, PITCH>(a, t * NZ);
 }
 
 
-template <int Q, int S, bool FORCE, int NZ, bool COMPACT = compact_face_rows<Q, S, FORCE>()>
+// PITCH: rows may carry padding (pz > nz) -- the kernel then handles a
+// partial last vector per row and writes the padding; lattices without
+// padding run the variant that has none of that code.
+template <int Q, int S, bool FORCE, int NZ, bool PITCH,
+          bool COMPACT = compact_face_rows<Q, S, FORCE>()>
 __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned t) {
   using St = Storage<S>;
   using T = typename St::T;
   using V = VSet<Q>;
   if constexpr (St::kBits == 16 && NZ == 2) {
-    step_vec_pairs<Q, S, FORCE, NZ, COMPACT>(a, t);
+    step_vec_pairs<Q, S, FORCE, NZ, COMPACT, PITCH>(a, t);
     return;
   }
   using R = typename St::R;
@@ -527,20 +588,29 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   if (pidx0 >= (unsigned)a.g.np) return;
   int x, y, z0;
   a.pdec(pidx0, x, y, z0);
-  if (z0 >= a.g.nz) return;                  // row padding
+  if constexpr (PITCH) {
+    if (z0 >= a.g.nz) {                      // row padding only
+      put_padding_vector<Q, S, NZ>(a, pidx0);
+      return;
+    }
+  }
   const unsigned idx0 = (unsigned)(x * a.g.ny + y) * (unsigned)a.g.nz + (unsigned)z0;
-  if (z0 + NZ > a.g.nz) {                    // the last nodes of a row (pitched rows)
-    face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, a.g.nz - z0, x, y, z0);
+  // Nodes of this vector inside the row: fewer than NZ in the last vector of
+  // a pitched row, whose other lanes are row padding -- loaded and stored
+  // with the vector (never a pull source, never observed) but not finished.
+  const int nv = PITCH && a.g.nz - z0 < NZ ? a.g.nz - z0 : NZ;
+  if (PITCH && nv < NZ && a.g.face[5] == LBM_BC_WALL_WITH_SPEED) {
+    face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, nv, NZ - nv, x, y, z0);
     return;
   }
   if (!lbm_in(x < a.g.nx && y < a.g.ny && pidx0 + NZ <= (unsigned)a.g.np &&
-              idx0 + NZ <= (unsigned)a.g.n))
+              idx0 + nv <= (unsigned)a.g.n))
     return;
   constexpr bool kCompact = COMPACT;
   bool row_in = x > 0 && x < a.g.nx - 1 && y > 0 && y < a.g.ny - 1;
   if constexpr (kCompact) {
     if (!row_in) {
-      face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, NZ, x, y, z0);
+      face_row_nodes<Q, S, FORCE>(a, idx0, pidx0, nv, NZ - nv, x, y, z0);
       return;
     }
     row_in = true;
@@ -548,7 +618,8 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   const R *face_rho = static_cast<const R *>(a.face_rho_in);
   R f[NZ][Q];
   if (row_in) {
-    const bool bottom = z0 == 0, top = z0 + NZ == a.g.nz;
+    // top: the row's last node is in this vector (lane nv - 1)
+    const bool bottom = z0 == 0, top = z0 + NZ >= a.g.nz;
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       constexpr int ez = V::ez(i);
@@ -577,10 +648,15 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
         for (int k = 1; k < NZ; ++k) f[k][i] = v[k - 1];
         f[0][i] = St::work(bottom ? static_cast<const T *>(a.p.zlo[i]) + pidx0 : ps - 1);
       } else {
+        // the row's last node (lane nv - 1) pulls the top face's value; in a
+        // partial vector the padding lanes after it take any value (a
+        // select per lane, not a store at a computed lane, which would put
+        // f in local memory)
+        const R e = St::work(top ? static_cast<const T *>(a.p.zhi[i]) + (pidx0 + (nv - 1))
+                                 : ps + NZ);
 #pragma unroll
-        for (int k = 0; k < NZ - 1; ++k) f[k][i] = v[k + 1];
-        f[NZ - 1][i] =
-            St::work(top ? static_cast<const T *>(a.p.zhi[i]) + (pidx0 + NZ - 1) : ps + NZ);
+        for (int k = 0; k < NZ - 1; ++k) f[k][i] = k == nv - 1 ? e : v[k + 1];
+        f[NZ - 1][i] = e;
       }
     });
     if (bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
@@ -589,9 +665,10 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
       zface_wws<Q, 5>(a.g, face_rho, x, y, a.g.nz - 1, f[NZ - 1]);
   } else if constexpr (!kCompact) {
     const T *fa = static_cast<const T *>(a.fa);
+    // (padding lanes repeat the row's last node; they are not finished)
 #pragma unroll
     for (int k = 0; k < NZ; ++k)
-      pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, face_rho, f[k]);
+      pull_general<Q, S, true>(fa, a.g, x, y, k < nv ? z0 + k : a.g.nz - 1, face_rho, f[k]);
   }
 
   unsigned bad = 0;
@@ -599,9 +676,10 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
   for (int k = 0; k < NZ; ++k) {
     const int z = z0 + k;
     // (a thread's nodes may straddle two force chunks: dense rows of any length)
-    finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z,
-                                    !row_in || z == 0 || z == a.g.nz - 1,
-                                    chunk_force<FORCE>(a, idx0 + k), bad);
+    if (k < nv)
+      finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z,
+                                      !row_in || z == 0 || z == a.g.nz - 1,
+                                      chunk_force<FORCE>(a, idx0 + k), bad);
   }
   report_bad(a.status, bad);
   if (a.fb == nullptr) return;
@@ -644,9 +722,10 @@ constexpr int vec_min_blocks() {
   return vec_reg_cap<Q, S, NZ, FORCE>() == 0 ? 0 : 65536 / (vec_reg_cap<Q, S, NZ, FORCE>() * TB);
 }
 
-template <int Q, int S, bool FORCE, int NZ, int TB>
-__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>())) k_step_vec(const __grid_constant__ StepArgs a) {
-  step_vec_body<Q, S, FORCE, NZ>(a, blockIdx.x * TB + threadIdx.x);
+template <int Q, int S, bool FORCE, int NZ, int TB, bool PITCH>
+__global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>()))
+    k_step_vec(const __grid_constant__ StepArgs a) {
+  step_vec_body<Q, S, FORCE, NZ, PITCH>(a, blockIdx.x * TB + threadIdx.x);
 }
 
 // Rows of odd length in 16-bit storage: thread k of a row takes the node pair
@@ -711,7 +790,7 @@ __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>()))
     if constexpr (NZ == 1)
       step_scalar_body<Q, S, FORCE>(sa, t0 + it * TB);
     else
-      step_vec_body<Q, S, FORCE, NZ>(sa, t0 + it * TB);
+      step_vec_body<Q, S, FORCE, NZ, true>(sa, t0 + it * TB);
   }
 }
 
@@ -1010,10 +1089,17 @@ struct StepLauncher {
   template <int NZ, int TB>
   static void go_vec(const StepArgs &a, bool force, cudaStream_t s) {
     const unsigned nb = blocks_for(a.g.np / NZ, TB);
-    if (force)
-      k_step_vec<Q, S, true, NZ, TB><<<nb, TB, 0, s>>>(a);
-    else
-      k_step_vec<Q, S, false, NZ, TB><<<nb, TB, 0, s>>>(a);
+    if (a.g.pz != a.g.nz) {
+      if (force)
+        k_step_vec<Q, S, true, NZ, TB, true><<<nb, TB, 0, s>>>(a);
+      else
+        k_step_vec<Q, S, false, NZ, TB, true><<<nb, TB, 0, s>>>(a);
+    } else {
+      if (force)
+        k_step_vec<Q, S, true, NZ, TB, false><<<nb, TB, 0, s>>>(a);
+      else
+        k_step_vec<Q, S, false, NZ, TB, false><<<nb, TB, 0, s>>>(a);
+    }
   }
   template <int NZ>
   static void go_nz(const StepArgs &a, bool force, int threads, cudaStream_t s) {
@@ -1042,15 +1128,15 @@ struct StepLauncher {
     if (nodes == LBM_STEP_ROWS) return go_tma(a, force, s);
     const bool odd_pairs = bits == 16 && a.g.pz % 2 == 1 && a.g.nz >= 3;
     if (nodes == 0) {
-      // measured on B200 at 512^3: 2 nodes per thread with 128-thread blocks
-      // is the fastest shape for every velocity set and storage, except
-      // D3Q19 in 16-bit storage, where 4 nodes per thread (register-capped)
-      // are -- unforced only: the forced 4-node kernel spills (see
-      // funlbm_b200.tune)
-      const int want = (bits == 16 && Q == 19 && !force) ? 4 : 2;
-      // (rows of odd length: one node per thread; the odd-row pair kernel
-      // is only a tuner candidate -- measured no faster in general)
-      nodes = step_shape_ok(want, a.g.pz, bits) ? want : step_shape_ok(2, a.g.pz, bits) ? 2 : 1;
+      // Measured on B200 (D3Q19): node pairs with 128-thread blocks are the
+      // fastest shape wherever rows allow them -- 512^3 FP32 3027 us (one
+      // node per thread 3066 us; 3035 against 3132 us over seconds under
+      // the power cap, where the pair kernel holds 1935 MHz and the other
+      // 1845), 512^3 fp16s 1869 us (4 nodes 1985 us).  Rows of odd length
+      // without pitch take one node per thread (on the walled 161x65x65 and
+      // 257x129x129 lattices also faster than pitched pairs); the odd-row
+      // pair kernel is a tuner candidate only.
+      nodes = step_shape_ok(2, a.g.pz, bits) ? 2 : 1;
       threads = threads ? threads : 128;
     }
     if (nodes == 2 && odd_pairs) {

@@ -355,6 +355,7 @@ class FlowD3(Flow):
     def fused_step(self, force, new_field=None, new_uniform=(0.0, 0.0, 0.0), keep=()):
         """One fused step on the lattice buffers (caller prepared `force`)."""
         self._lat.step(force)
+        self._loaded_fused = False
         self._last_force = (force, (new_field, tuple(new_uniform)))
         self._keep = keep
         self._obs_valid = False
@@ -525,27 +526,67 @@ class FlowD3(Flow):
         return {"f": v[0:3], "u": v[3:6], "rho": v[6:9]}
 
     def dump_checkpoint(self, group=None, *args, **kwargs):
-        """flow/base.py:208-211: ``f``; also ``FOL`` (not in the reference's
-        file), the force the end-of-step moments include, so that a loaded
-        state continues exactly as the saved run would have."""
-        if group is not None:
-            group.create_dataset("f", data=self.f.cpu().numpy(), compression="gzip",
-                                 compression_opts=9)
-            group.create_dataset("FOL", data=self.FOL.cpu().numpy(), compression="gzip",
-                                 compression_opts=9)
+        """flow/base.py:208-211: ``f``; also, not in the reference's file,
+        ``FOL`` (the force the end-of-step moments include) and, while the
+        state lives in the lattice buffers, the stored populations themselves
+        (``populations``: dense [q][x][y][z] in the storage's type, 16-bit
+        forms as their raw bits; ``storage_code``; ``face_rho``), so that a
+        loaded state continues bit for bit as the saved run would have: the
+        buffers hold f - w_i, which f rounded to float32 does not determine."""
+        if group is None:
+            return
+        group.create_dataset("f", data=self.f.cpu().numpy(), compression="gzip",
+                             compression_opts=9)
+        group.create_dataset("FOL", data=self.FOL.cpu().numpy(), compression="gzip",
+                             compression_opts=9)
+        if self._mode == "fused":
+            lat = self._lat
+            X, Y, Z = self.shape
+            pop = lat.buf[lat.cur].view(lat.q, X * Y, lat.pz)[:, :, :Z].contiguous()
+            if pop.element_size() == 2:
+                pop = pop.view(torch.int16)
+            group.create_dataset("populations", data=pop.view(lat.q, -1).cpu().numpy(),
+                                 compression="gzip", compression_opts=9)
+            group.create_dataset("storage_code", data=[_lib.STORAGE[lat.storage]])
+            if lat.needs_face_rho:
+                group.create_dataset("face_rho", data=lat.face_rho[lat.cur].cpu().numpy())
 
     def load_checkpoint(self, group=None, *args, **kwargs):
         """flow/base.py:213-216 (with the reference's tensor-construction
-        TypeError fixed): f, then the moments; FOL when the file has it."""
+        TypeError fixed): f, then the moments; FOL when the file has it; the
+        stored populations when the file has them for this lattice's storage
+        (the state then continues in the fused form exactly)."""
         if group is None:
             return
-        if getattr(self, "_fp64", False):
+        fp64 = getattr(self, "_fp64", False)
+        pop, code = group.get("populations"), group.get("storage_code")
+        exact = (pop is not None and code is not None and self._lat is not None
+                 and int(np.asarray(code[:]).reshape(-1)[0]) == _lib.STORAGE[self.storage]
+                 and tuple(np.asarray(pop[:]).shape) == (self.q, self.n))
+        if fp64 and not exact:
             self._fp64_only_fused("load_checkpoint")
-        self.f = torch.tensor(np.asarray(group.get("f")[:]), dtype=torch.float32, device=self.device)
+        dt = torch.float64 if fp64 else torch.float32
+        self.f = torch.tensor(np.asarray(group.get("f")[:]), dtype=dt, device=self.device)
         fol = group.get("FOL")
         if fol is not None:
             self.FOL = torch.tensor(np.asarray(fol[:]), dtype=torch.float32, device=self.device)
         self.update_u_rou()
+        if not exact:
+            return
+        # the populations the next step streams from, as the saved run held
+        # them; f / rho / u above stay the observed state until that step
+        lat = self._lat
+        lat.allocate()
+        X, Y, Z = self.shape
+        src = torch.from_numpy(np.ascontiguousarray(np.asarray(pop[:])))
+        dst = lat.buf[lat.cur].view(lat.q, X * Y, lat.pz)[:, :, :Z]
+        dst.copy_(src.view(dst.dtype).view(lat.q, X * Y, Z).to(self.device))
+        fr = group.get("face_rho")
+        if lat.needs_face_rho and fr is not None:
+            lat.face_rho[lat.cur].copy_(torch.from_numpy(np.asarray(fr[:])).to(self.device))
+        self._mode = "fused"
+        self._obs_valid = True
+        self._loaded_fused = True       # the next step enters this state's FOL
 
 
 def face_planes(rho3):

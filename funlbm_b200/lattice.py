@@ -1,10 +1,12 @@
 """Device state of one lattice on the fused path, over the C ABI.
 
 A ``Lattice`` owns two population buffers in structure-of-arrays layout
-``[q][x][y][z]`` (storage type fp32 / fp16s / bf16s) and ping-pongs between
+``[q][x][y][z]`` and ping-pongs between
 them: ``buf[cur]`` holds the post-collision populations the next step streams
 from, ``buf[cur ^ 1]`` the ones the last step streamed from (kept for
-observation).  Everything numeric runs in ``liblbm_b200.so``.
+observation).  fp32, fp16s and bf16s buffers hold the deviation d = f - w_i
+of each population from its weight (float32, float16, bfloat16); fp64
+buffers hold f.  Everything numeric runs in ``liblbm_b200.so``.
 """
 from __future__ import annotations
 
@@ -23,6 +25,23 @@ BYTES = {"fp32": 4, "fp16s": 2, "bf16s": 2, "fp64": 8}
 # elements of the widest vector (16 bytes) the step moves per thread: the
 # population rows are pitched to a multiple of it
 VECTOR_ELEMS = {"fp32": 4, "fp16s": 8, "bf16s": 8, "fp64": 2}
+
+
+# 16-bit lattices of at least this many nodes pitch rows of odd length
+PITCH_MIN_NODES = 1 << 24
+
+
+def default_pitch(shape, storage):
+    """Whether a lattice pitches its population rows unless told otherwise:
+    16-bit storage, rows of odd length, at least 2^24 nodes.  Measured on
+    B200 (D3Q19 fp16s): pitched rows let node pairs run and win 9 % at 257^3
+    (322 against 351 us per step on dense rows); on the walled 161x65x65
+    and 257x129x129 lattices one node per thread on dense rows wins (23.0
+    against 27.0 us, 162.6 against 173.2 us); in FP32 dense rows win
+    (257^3: 435 us dense, 448 us pitched)."""
+    shape = tuple(int(s) for s in shape)
+    return (BYTES[storage] == 2 and shape[2] % 2 == 1
+            and shape[0] * shape[1] * shape[2] >= PITCH_MIN_NODES)
 
 
 def row_pitch(nz, storage):
@@ -72,13 +91,16 @@ class Lattice:
     """One lattice: descriptor, population buffers, face-density planes."""
 
     def __init__(self, q, shape, faces, tau, storage="fp32", face_uw=None, re_mu=0.0,
-                 device="cuda", allocate=True, pitch=True):
+                 device="cuda", allocate=True, pitch=None):
         if storage not in STORAGE_DTYPE:
             raise ValueError("unknown storage %r (fp32, fp16s, bf16s)" % (storage,))
         self.q = int(q)
         self.shape = tuple(int(s) for s in shape)
         self.n = self.shape[0] * self.shape[1] * self.shape[2]
-        # population rows pitched to the vector width (pitch=False: dense rows)
+        # population rows pitched to the vector width (pitch=False: dense
+        # rows; None: default_pitch)
+        if pitch is None:
+            pitch = default_pitch(self.shape, storage)
         self.pz = row_pitch(self.shape[2], storage) if pitch else self.shape[2]
         self.np = self.shape[0] * self.shape[1] * self.pz
         self.storage = storage
@@ -122,8 +144,11 @@ class Lattice:
 
     # -- memory ------------------------------------------------------------
     @staticmethod
-    def bytes_needed(q, shape, storage="fp32"):
-        n = int(shape[0]) * int(shape[1]) * row_pitch(shape[2], storage)
+    def bytes_needed(q, shape, storage="fp32", pitch=None):
+        if pitch is None:
+            pitch = default_pitch(shape, storage)
+        pz = row_pitch(shape[2], storage) if pitch else int(shape[2])
+        n = int(shape[0]) * int(shape[1]) * pz
         planes = 2 * (shape[1] * shape[2] + shape[0] * shape[2] + shape[0] * shape[1])
         return 2 * q * n * BYTES[storage] + 2 * REAL_DTYPE[storage].itemsize * planes
 
@@ -166,7 +191,7 @@ class Lattice:
         X, Y, Z = self.shape
         dst = self.buf[self.cur].view(self.q, X * Y, self.pz)[:, :, :Z]
         src = a.reshape(self.q, X * Y, Z)
-        if self.storage in ("fp32", "fp64"):
+        if self.storage == "fp64":
             dst.copy_(src)
         else:
             w = weights_tensor(self.q, self.device)

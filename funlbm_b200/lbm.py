@@ -451,7 +451,8 @@ class LBMD3(LBMBase):
         ``_fused_step``, or packed with other lattices by a server).  With
         launch=False only the description is computed (nothing is issued)."""
         fl = self.flow
-        entering = fl._mode != "fused"
+        # (a checkpoint restored in the fused form counts as entering it)
+        entering = fl._mode != "fused" or getattr(fl, "_loaded_fused", False)
         fl.enter_fused()
         lat = fl.lattice
         g_new = self.body_force

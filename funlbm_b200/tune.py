@@ -41,14 +41,11 @@ def shape_ok(nodes, pz, bits, nz=None):
 
 
 def default_shape(q, storage, pz, forced=False):
-    """The launch shape lbm_flow_step uses when none is set (measured best at
-    512^3): 2 nodes per thread with 128 threads, 4 for unforced D3Q19 in
-    16-bit storage, one node per thread where rows allow no vector."""
-    bits = STORAGE_BITS[storage]
-    want = 4 if (bits == 16 and q == 19 and not forced) else 2
-    for nodes in (want, 2):
-        if pz % nodes == 0 and pz >= 2 * nodes:
-            return (nodes, 128)
+    """The launch shape lbm_flow_step uses when none is set (measured best on
+    B200 at 512^3 in FP32 and fp16s): node pairs with 128 threads where the
+    rows allow them, else one node per thread."""
+    if pz % 2 == 0 and pz >= 4:
+        return (2, 128)
     return (1, 256)
 
 

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 CHILD = r"""
-import hashlib, json, os, sys
+import hashlib, itertools, json, os, sys
 import numpy as np
 root, checked = sys.argv[1], sys.argv[2] == "1"
 sys.path.insert(0, root)
@@ -26,6 +26,7 @@ import torch
 from funlbm_b200 import _lib, build
 build.build(checked=checked)
 lib = _lib.load()
+assert lib._name.endswith("liblbm_b200_checked.so" if checked else "liblbm_b200.so"), lib._name
 from funlbm_b200.lattice import Lattice, make_force, tau_float32
 from funlbm_b200.lbm import LBMD3, Config
 from funlbm_b200.tune import CANDIDATES, STORAGE_BITS, shape_ok
@@ -51,9 +52,11 @@ for storage in ("fp32", "fp16s", "fp64"):
         f0 = smooth_f0(q, shape, 0.04, q)
         f0 = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda", dtype=dt)
         bits = STORAGE_BITS[storage]
-        for nodes, threads in CANDIDATES[bits]:
-            lat = Lattice(q, shape, [1200, 11000, 11000, 1200, 1201, 1201], tau_float32(0.07),
-                          storage=storage, face_uw=[(0.01, 0.0, -0.01)] * 6, device="cuda")
+        for (nodes, threads), pitch, zf in itertools.product(
+                CANDIDATES[bits], (False, True), ((1201, 1201), (1200, 11000))):
+            lat = Lattice(q, shape, [1200, 11000, 11000, 1200, *zf], tau_float32(0.07),
+                          storage=storage, face_uw=[(0.01, 0.0, -0.01)] * 6, device="cuda",
+                          pitch=pitch)
             if not shape_ok(nodes, lat.pz, bits, shape[2]):
                 continue
             lat.set_launch_shape(nodes, threads)
@@ -62,8 +65,9 @@ for storage in ("fp32", "fp16s", "fp64"):
                 lat.step(force)
             f = torch.empty(q * lat.n, device="cuda", dtype=dt)
             lat.observe(force, f=f)
-            out["lat_%s_q%d_%d_%d" % (storage, q, nodes, threads)] = h(f)
-            out["stats_%s_q%d_%d_%d" % (storage, q, nodes, threads)] = h(lat.stats(force))
+            key = "%s_q%d_%d_%d_%d_%d" % (storage, q, nodes, threads, pitch, zf[0])
+            out["lat_" + key] = h(f)
+            out["stats_" + key] = h(lat.stats(force))
 parts = [{"type": "sphere", "r": 3, "rou": 1.4, "coord": {"center": [2.4, 8.0, 9.1]}},
          {"type": "ellipsoid", "a": 3, "b": 2, "c": 2.5, "rou": 0.7,
           "coord": {"center": [12.5, 11.3, 7.6], "alpha": 0.3, "beta": -0.5, "gamma": 0.2}}]
@@ -86,8 +90,9 @@ print(json.dumps({"faults": int(lib.lbm_debug_bounds_faults(0)), "hashes": out})
 
 
 def _child(checked):
+    env = dict(os.environ, FUNLBM_B200_CHECKED="1" if checked else "0")
     r = subprocess.run([sys.executable, "-c", CHILD, ROOT, "1" if checked else "0"],
-                       capture_output=True, text=True, timeout=1200)
+                       capture_output=True, text=True, timeout=1200, env=env)
     assert r.returncode == 0, r.stderr[-3000:]
     return json.loads(r.stdout.strip().splitlines()[-1])
 

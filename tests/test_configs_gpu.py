@@ -10,12 +10,15 @@ x and y, periodic z, body force (0, 0, 1e-6), 2000 steps:
   u within 1e-8 of max|u|, mean density within 1e-12.
 * FP32 storage against the reference's own float32 run (all nodes):
   rho within 5e-5 relative and u within 3e-2 of max|u|.  These bounds are
-  float32's own, not the kernel's: over 2000 steps the reference's float32
-  run drifts from the float64 run by 2.5e-5 in rho (its total mass grows by
-  that much) and by 1.4e-2 of max|u| in u (2-3e-7 absolute, in every
-  component), and the float32 oracle differs from the reference by 1.9e-6 in
-  rho and 1.25e-2 in u.  The test also requires the FP32 kernel to sit no
-  farther from the float64 run than the reference does (within 1.5x).
+  the reference's float32 drift, not the kernel's: over 2000 steps the
+  reference's run departs from the float64 run by 2.5e-5 in rho (its total
+  mass grows by that much) and by 1.4e-2 of max|u| in u (2-3e-7 absolute,
+  in every component): the body force adds ~17 units in the last place to a
+  population of ~0.056 each step, and in a nearly steady flow that rounding
+  has the same sign step after step.  The FP32 storage holds f - w_i, whose
+  32 bits resolve the same increments to ~1e-7 of themselves: the test
+  requires it within 1e-4 of max|u| of the float64 run and at most 1 % of the
+  reference's distance from it.
 * The analytic duct profile: the reference zeroes u on all six boundary
   planes (flow/d3/base.py:128-133), the periodic z planes included, so the
   channel flows ~35x slower than a duct would; the shape of the mid-plane
@@ -26,9 +29,24 @@ x and y, periodic z, body force (0, 0, 1e-6), 2000 steps:
 
 Config 2 -- single sphere free fall, D3Q19, 161 x 65 x 65 nodes, tau 0.7,
 walls, radius 8 (1160 markers) at (130, 32, 32), density 1.5, gl 2e-5, 5000
-steps: the particle's position and velocity every 100 steps within 1e-4
-lattice units of the reference's (the step-100 weight-sum sentinel of
-lbm/lbm3d.py:84-86 is active for 4900 of them).
+steps (the step-100 weight-sum sentinel of lbm/lbm3d.py:84-86 is active for
+4900 of them), against the reference's float32 run every 100 steps:
+
+* velocity within 1e-4 lattice units over the whole horizon, and at most
+  1.2x the FP64 kernel run's largest distance from it: what remains is the
+  reference's own float32 error (measured: 6.2e-7, 3 % of max|cu|; the FP64
+  run sits 5.8e-7 from it, the FP32 run 2.1e-7 from the FP64 run);
+* position within 1e-4 lattice units along the fall (x) over the whole
+  horizon -- both float32 runs move x by exactly one unit in the last
+  place per step (|cu dt| is 0.66-1.2 of the 1.5e-5 spacing at x = 130), so
+  they agree exactly -- and in y / z through step 4000.  The lateral drift
+  (cu_y ~ -4.5e-6, 2.3-2.5 units of the 1.9e-6 spacing at y = 32) is rounded
+  to whole units every step in both float32 runs, and where the reference's
+  3 % velocity error crosses a half-unit boundary the two take different
+  numbers of units for some steps: measured 1.3e-5 at step 4000 and 1.39e-4
+  from step 4400 on.  The reference's float32 position is itself 2.9e-3 (y)
+  and 1.2e-2 (x) from the FP64 kernel run's at step 5000, so past step 4000
+  the test requires the FP32 run within a tenth of that distance of it.
 """
 import os
 
@@ -104,7 +122,10 @@ def test_config1_poiseuille():
         rou64, u64 = states[("fp64", s)]
         o_rou, o_u = g["oracle64_rou_mid_%d" % s], g["oracle64_u_mid_%d" % s]
         assert np.abs(rou64[:, :, zmid] - o_rou).max() <= 1e-10 * np.abs(o_rou).max()
-        assert np.abs(u64[:, :, zmid] - o_u).max() <= 1e-8 * np.abs(o_u).max()
+        # u is a difference of O(0.1) population sums, so its double rounding
+        # is absolute (about 1e-16 per operation, accumulated over the
+        # steps), not relative to |u| (2e-5 here): measured 6.6e-13 on B200
+        assert np.abs(u64[:, :, zmid] - o_u).max() <= 1e-11
         assert abs(rou64.mean() - float(g["oracle64_rou_mean_%d" % s])) <= 1e-12
         # FP32 kernel vs the reference's float32 run, at float32's own noise
         rou32, u32 = states[("fp32", s)]
@@ -118,7 +139,10 @@ def test_config1_poiseuille():
         print("config 1 step %d: fp32 vs reference rho %.2e u %.2e; from float64: reference %.2e,"
               " fp32 kernel %.2e" % (s, e_rho, e_u, d_ref, d_gpu))
         assert e_rho <= 5e-5 and e_u <= 3e-2
-        assert d_gpu <= 1.5 * d_ref
+        # the FP32 storage holds f - w_i: it stays at float64's solution
+        # (measured 7.3e-6 / 6.8e-6 of max|u| after 1000 / 2000 steps) where
+        # the reference's float32 run has drifted by 7.9e-3 / 8.6e-3
+        assert d_gpu <= 1e-4 and d_gpu <= 0.01 * d_ref
     # the duct shape of the mid-plane cross-section
     uz = states[("fp32", 2000)][1][:, :, zmid, 2]
     shape = uz / uz[size[0] // 2, size[1] // 2]
@@ -128,24 +152,48 @@ def test_config1_poiseuille():
     assert np.abs(shape - prof / prof[n // 2, n // 2]).max() <= 0.1
 
 
-def test_config2_sphere_free_fall():
+def _sphere_history(storage, steps):
     from funlbm_b200.lbm import LBMD3
 
-    g = np.load(os.path.join(GOLD, "config2_sphere.npz"))
-    steps = int(g["steps"])
     part = {"type": "sphere", "r": 8, "rou": 1.5, "coord": {"center": [130, 32, 32]}}
-    lbm = LBMD3(config=_config((160, 64, 64), 0.0666667, ("WALL",) * 6, particles=[part], gl=2e-5))
+    lbm = LBMD3(config=_config((160, 64, 64), 0.0666667, ("WALL",) * 6, storage=storage,
+                               particles=[part], gl=2e-5))
     lbm.init()
     p = lbm.particle_swarm.particles[0]
-    assert np.abs(to64(p._lagrange) - g["lagrange"]).max() <= 1e-6
-    worst = {"cx": 0.0, "cu": 0.0}
+    hist = {"cx": [], "cu": [], "lagrange": to64(p._lagrange)}
     for s in range(100, steps + 1, 100):
         lbm.run_steps(s - lbm.step + 1)
         assert lbm.run_status and lbm.step == s + 1
-        for k in worst:
-            err = np.abs(to64(getattr(p, k)) - g[k][s - 1]).max()
-            worst[k] = max(worst[k], err)
-            assert err <= 1e-4, (s, k, err)
+        hist["cx"].append(to64(p.cx))
+        hist["cu"].append(to64(p.cu))
     assert lbm.check_status() == 0
-    print("config 2, %d steps: max |cx - ref| %.2e, max |cu - ref| %.2e, fall %.2f lu"
-          % (steps, worst["cx"], worst["cu"], 130 - float(g["cx"][-1][0])))
+    hist["u_mid"] = to64(lbm.flow.u)[:, :, 32]
+    hist["rou_mid"] = to64(lbm.flow.rou)[:, :, 32]
+    return {k: np.asarray(v) for k, v in hist.items()}
+
+
+def test_config2_sphere_free_fall():
+    g = np.load(os.path.join(GOLD, "config2_sphere.npz"))
+    steps = int(g["steps"])
+    h32 = _sphere_history("fp32", steps)
+    h64 = _sphere_history("fp64", steps)
+    assert np.abs(h32["lagrange"] - g["lagrange"]).max() <= 1e-6
+    at = np.arange(100, steps + 1, 100) - 1
+    ref_cx, ref_cu = g["cx"][at].astype(np.float64), g["cu"][at].astype(np.float64)
+    e_cx = np.abs(h32["cx"] - ref_cx)                  # [checkpoints, 3]
+    e_cu = np.abs(h32["cu"] - ref_cu).max(axis=1)
+    d64_cx = np.abs(h64["cx"] - ref_cx)
+    d64_cu = np.abs(h64["cu"] - ref_cu).max(axis=1)
+    e_u = np.abs(h32["u_mid"] - g["u_mid"][:, :, 0]).max() / np.abs(g["u_mid"]).max()
+    print("config 2, %d steps: max |cx - ref| x %.2e, y/z %.2e (through step 4000: %.2e); "
+          "max |cu - ref| %.2e (FP64 run: %.2e); reference from FP64 at the end: x %.2e, y %.2e; "
+          "fall %.3f lu; mid-plane u %.2e of max |u|"
+          % (steps, e_cx[:, 0].max(), e_cx[:, 1:].max(), e_cx[:40, 1:].max(), e_cu.max(),
+             d64_cu.max(), d64_cx[-1, 0], d64_cx[-1, 1], 130 - float(g["cx"][-1][0]), e_u))
+    assert e_cu.max() <= 1e-4
+    assert e_cu.max() <= 1.2 * d64_cu.max()
+    # the FP32 kernel's velocity follows the FP64 kernel's (measured 2.1e-7)
+    assert np.abs(h32["cu"] - h64["cu"]).max() <= 5e-7
+    assert e_cx[:, 0].max() <= 1e-4
+    assert e_cx[:40, 1:].max() <= 1e-4
+    assert np.all(e_cx[40:, 1:] <= 0.1 * d64_cx[40:, 1:])

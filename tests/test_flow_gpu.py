@@ -487,16 +487,19 @@ def test_row_staged_wait_timeout_sets_status():
 def test_pitched_rows_agree_bitwise(q, storage):
     """Population rows pitched to the vector width (rows of 13 and 33 nodes
     stored in rows of 16 / 36 / 40 elements): every launch shape on the pitched
-    buffers -- vectors over full groups, the per-node path for the last nodes
-    of each row -- gives the bits of one node per thread on dense rows, with
-    WALL_WITH_SPEED z faces, walls and chunked force fields."""
+    buffers -- vectors over full groups, a partial last vector per row whose
+    padding lanes are not finished (or the per-node path under a
+    WALL_WITH_SPEED top face) -- gives the bits of one node per thread on
+    dense rows, with WALL / PERIODICAL / WALL_WITH_SPEED z faces, walls and
+    chunked force fields."""
     from funlbm_b200.lattice import Lattice, make_force, tau_float32
     from funlbm_b200.tune import CANDIDATES, STORAGE_BITS, shape_ok
 
     rng = np.random.default_rng(50 + q)
     bits = STORAGE_BITS[storage]
     dt = torch.float64 if storage == "fp64" else torch.float32
-    for shape in ((9, 8, 13), (7, 6, 33)):
+    for shape, zfaces in (((9, 8, 13), (1201, 1201)), ((7, 6, 33), (1201, 1201)),
+                          ((9, 8, 13), (1200, 11000)), ((7, 6, 33), (11000, 1200))):
         n = shape[0] * shape[1] * shape[2]
         nch = (n + 31) // 32
         kind = rng.integers(0, 4, nch)
@@ -510,7 +513,7 @@ def test_pitched_rows_agree_bitwise(q, storage):
         F_old = torch.tensor(f_old.reshape(-1), device="cuda", dtype=dt)
         F_new = torch.tensor(f_new.reshape(-1), device="cuda", dtype=dt)
         force = make_force((0, 0, 0), (2e-6, 0, 0), F_old, F_new, ch_old, ch_new)
-        codes = [1200, 11000, 11000, 1200, 1201, 1201]
+        codes = [1200, 11000, 11000, 1200, *zfaces]
         uw = (0.02 * rng.standard_normal((6, 3))).tolist()
         f0 = smooth_f0(q, shape, 0.04, q + 7)
         f0_soa = torch.tensor(np.ascontiguousarray(np.moveaxis(f0, -1, 0)), device="cuda",
@@ -535,4 +538,4 @@ def test_pitched_rows_agree_bitwise(q, storage):
         ref = results[(False, 1, 256, shape[2])]
         assert any(k[0] and k[1] > 1 for k in results)
         for k, v in results.items():
-            assert np.array_equal(v, ref), (shape, k, np.abs(v - ref).max())
+            assert np.array_equal(v, ref), (shape, zfaces, k, np.abs(v - ref).max())
