@@ -830,7 +830,7 @@ __device__ __forceinline__ float sm_elem(const typename Storage<S>::T *p) {
   if constexpr (Storage<S>::kBits == 32)
     return *p;
   else if constexpr (S == LBM_STORAGE_FP16S)
-    return __half2float(*p);
+    return Storage<S>::cvt(*p);
   else
     return __bfloat162float(*p);
 }

@@ -561,7 +561,7 @@ class FlowD3(Flow):
         fp64 = getattr(self, "_fp64", False)
         pop, code = group.get("populations"), group.get("storage_code")
         exact = (pop is not None and code is not None and self._lat is not None
-                 and int(np.asarray(code[:]).reshape(-1)[0]) == _lib.STORAGE[self.storage]
+                 and int(np.asarray(code[:]).reshape(-1)[0]) == _lib.STORAGE[self._lat.storage]
                  and tuple(np.asarray(pop[:]).shape) == (self.q, self.n))
         if fp64 and not exact:
             self._fp64_only_fused("load_checkpoint")

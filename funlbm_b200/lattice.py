@@ -5,8 +5,8 @@ A ``Lattice`` owns two population buffers in structure-of-arrays layout
 them: ``buf[cur]`` holds the post-collision populations the next step streams
 from, ``buf[cur ^ 1]`` the ones the last step streamed from (kept for
 observation).  fp32, fp16s and bf16s buffers hold the deviation d = f - w_i
-of each population from its weight (float32, float16, bfloat16); fp64
-buffers hold f.  Everything numeric runs in ``liblbm_b200.so``.
+of each population from its weight (float32, float16 scaled by 2^12,
+bfloat16); fp64 buffers hold f.  Everything numeric runs in ``liblbm_b200.so``.
 """
 from __future__ import annotations
 
@@ -22,6 +22,8 @@ BC = {"PERIODICAL": 11000, "WALL": 1200, "WALL_WITH_SPEED": 1201, "NON_EQUILIBRI
 STORAGE_DTYPE = {"fp32": torch.float32, "fp16s": torch.float16, "bf16s": torch.bfloat16,
                  "fp64": torch.float64}
 BYTES = {"fp32": 4, "fp16s": 2, "bf16s": 2, "fp64": 8}
+# fp16s buffers hold (f - w) * FP16_SCALE (kept out of float16's subnormals)
+FP16_SCALE = 4096.0
 # elements of the widest vector (16 bytes) the step moves per thread: the
 # population rows are pitched to a multiple of it
 VECTOR_ELEMS = {"fp32": 4, "fp16s": 8, "bf16s": 8, "fp64": 2}
@@ -195,7 +197,10 @@ class Lattice:
             dst.copy_(src)
         else:
             w = weights_tensor(self.q, self.device)
-            dst.copy_((src - w[:, None, None]).to(STORAGE_DTYPE[self.storage]))
+            d = src - w[:, None, None]
+            if self.storage == "fp16s":
+                d = d * FP16_SCALE
+            dst.copy_(d.to(STORAGE_DTYPE[self.storage]))
 
     def step(self, force=None, obs=None):
         nxt = self.cur ^ 1

@@ -163,10 +163,11 @@ class LBMBase:
 
     def _quiet_steps(self, last):
         """How many steps from self.step on are plain fused steps: not the
-        first (it enters the fused form), no logging, no checkpoint, not the
-        last one."""
+        first (it enters the fused form, or the state a checkpoint restored
+        in it), no logging, no checkpoint, not the last one."""
         gs = int(self.config.graph_steps or 0)
-        if gs < 2 or self.step <= 1 or not self._use_fused() or self.flow._mode != "fused":
+        if (gs < 2 or self.step <= 1 or not self._use_fused() or self.flow._mode != "fused"
+                or getattr(self.flow, "_loaded_fused", False)):
             return 0
         s = self.step
         L = max(1, int(self.config.log_per_steps))

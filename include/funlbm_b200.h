@@ -60,7 +60,7 @@ extern "C" {
 #define LBM_STORAGE_FP32 0  /* float32 of (f_i - w_i), collided in float32: the */
                             /* reference's type, stored as the deviation so a   */
                             /* low-Mach flow keeps its velocity bits            */
-#define LBM_STORAGE_FP16S 1 /* float16 of (f_i - w_i), collided in float32       */
+#define LBM_STORAGE_FP16S 1 /* float16 of 4096 (f_i - w_i), collided in float32 */
 #define LBM_STORAGE_BF16S 2 /* bfloat16 of (f_i - w_i), collided in float32      */
 #define LBM_STORAGE_FP64 3  /* float64 populations and float64 arithmetic: the  */
                             /* comparison run of the storage error figures (the */

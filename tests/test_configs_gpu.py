@@ -184,7 +184,7 @@ def test_config2_sphere_free_fall():
     e_cu = np.abs(h32["cu"] - ref_cu).max(axis=1)
     d64_cx = np.abs(h64["cx"] - ref_cx)
     d64_cu = np.abs(h64["cu"] - ref_cu).max(axis=1)
-    e_u = np.abs(h32["u_mid"] - g["u_mid"][:, :, 0]).max() / np.abs(g["u_mid"]).max()
+    e_u = np.abs(h32["u_mid"] - g["u_mid"]).max() / np.abs(g["u_mid"]).max()
     print("config 2, %d steps: max |cx - ref| x %.2e, y/z %.2e (through step 4000: %.2e); "
           "max |cu - ref| %.2e (FP64 run: %.2e); reference from FP64 at the end: x %.2e, y %.2e; "
           "fall %.3f lu; mid-plane u %.2e of max |u|"
