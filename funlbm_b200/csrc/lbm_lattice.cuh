@@ -155,6 +155,7 @@ struct Storage<LBM_STORAGE_FP32> {
   using R = float;   // arithmetic type of the kernels
   static constexpr int kBits = 32;
   static constexpr bool kDev = true;
+  static constexpr int kShift = 0;   // working value = d * 2^kShift
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
   __device__ __forceinline__ static float cvt(T v) { return v; }
   __device__ __forceinline__ static float work(const T *p) { return __ldg(p); }
@@ -168,7 +169,10 @@ struct Storage<LBM_STORAGE_FP32> {
 // (spacing 6e-8: a 90 % velocity error measured over 3000 steps of the
 // 32-ellipsoid case).  Scaled, deviations from 1.5e-8 up to 16 keep the full
 // 11-bit significand; populations stay in [0, 1], so |d| < 1.  The scale is
-// a power of two: the scaling itself is exact.
+// a power of two: the scaling itself is exact.  The fused step keeps the
+// scaled value as its working value (kShift): the moments unscale their sums
+// and the collision and forcing carry the scale in their weight constants,
+// so no element is multiplied on load or store.
 constexpr float kFp16Scale = 4096.f;
 constexpr float kFp16Unscale = 1.f / 4096.f;
 
@@ -178,12 +182,11 @@ struct Storage<LBM_STORAGE_FP16S> {
   using R = float;
   static constexpr int kBits = 16;
   static constexpr bool kDev = true;
+  static constexpr int kShift = 12;
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
-  __device__ __forceinline__ static float cvt(T v) { return __half2float(v) * kFp16Unscale; }
-  __device__ __forceinline__ static float work(const T *p) {
-    return __half2float(__ldg(p)) * kFp16Unscale;
-  }
-  __device__ __forceinline__ static void put(T *p, float v) { *p = __float2half_rn(v * kFp16Scale); }
+  __device__ __forceinline__ static float cvt(T v) { return __half2float(v); }
+  __device__ __forceinline__ static float work(const T *p) { return __half2float(__ldg(p)); }
+  __device__ __forceinline__ static void put(T *p, float v) { *p = __float2half_rn(v); }
   __device__ __forceinline__ static float load(const T *p, float w) {
     return w + __half2float(__ldg(p)) * kFp16Unscale;
   }
@@ -197,6 +200,7 @@ struct Storage<LBM_STORAGE_BF16S> {
   using R = float;
   static constexpr int kBits = 16;
   static constexpr bool kDev = true;
+  static constexpr int kShift = 0;
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
   __device__ __forceinline__ static float cvt(T v) { return __bfloat162float(v); }
   __device__ __forceinline__ static float work(const T *p) { return __bfloat162float(__ldg(p)); }
@@ -217,6 +221,7 @@ struct Storage<LBM_STORAGE_FP64> {
   using R = double;
   static constexpr int kBits = 64;
   static constexpr bool kDev = false;
+  static constexpr int kShift = 0;
   __device__ __forceinline__ static T raw(const T *p) { return __ldg(p); }
   __device__ __forceinline__ static double cvt(T v) { return v; }
   __device__ __forceinline__ static double work(const T *p) { return __ldg(p); }
@@ -236,8 +241,7 @@ template <>
 __device__ __forceinline__ float2 work2<LBM_STORAGE_FP16S>(unsigned word) {
   __half2 h;
   memcpy(&h, &word, 4);
-  const float2 v = __half22float2(h);
-  return make_float2(v.x * kFp16Unscale, v.y * kFp16Unscale);
+  return __half22float2(h);
 }
 template <>
 __device__ __forceinline__ float2 work2<LBM_STORAGE_BF16S>(unsigned word) {
@@ -247,7 +251,7 @@ template <int S>
 __device__ __forceinline__ unsigned put2(float a, float b);
 template <>
 __device__ __forceinline__ unsigned put2<LBM_STORAGE_FP16S>(float a, float b) {
-  const __half2 h = __floats2half2_rn(a * kFp16Scale, b * kFp16Scale);
+  const __half2 h = __floats2half2_rn(a, b);
   unsigned word;
   memcpy(&word, &h, 4);
   return word;
@@ -365,7 +369,8 @@ __device__ __forceinline__ bool on_any_face(const Geom &g, int x, int y, int z) 
 // enters; -1 means none.  `face_rho` is consulted only for WALL_WITH_SPEED
 // faces (density of the previous step at this face node).
 // WORK: return the storage's working value (d for the shifted forms) instead
-// of f; the WALL_WITH_SPEED correction is the same in both.
+// of f; the WALL_WITH_SPEED correction is the same in both (in working
+// units: times 2^kShift).
 template <int Q, int S, int I, bool WORK = false>
 __device__ __forceinline__ typename Storage<S>::R pull_one(
     const typename Storage<S>::T *__restrict__ fa, const Geom &g, int x, int y, int z,
@@ -411,7 +416,8 @@ __device__ __forceinline__ typename Storage<S>::R pull_one(
   const long long src = ((long long)sx * g.ny + sy) * g.pz + sz;
   const R w_sd = sd == I ? V::template wr<R>(I) : V::template wr<R>(V::rev(I));
   if constexpr (WORK)
-    return Storage<S>::work(fa + (long long)sd * g.np + src) - corr;
+    return Storage<S>::work(fa + (long long)sd * g.np + src) -
+           corr * R(1 << Storage<S>::kShift);
   else
     return Storage<S>::load(fa + (long long)sd * g.np + src, w_sd) - corr;
 }
@@ -465,7 +471,7 @@ struct StepPlanes {
 // WALL_WITH_SPEED correction of the directions entering through z face FC
 // (4 = bottom, 5 = top) at a node of an interior row, applied after the
 // plain bounce-back pull: the same expression as pull_one's.
-template <int Q, int FC, typename R>
+template <int Q, int FC, int SH = 0, typename R>
 __device__ __forceinline__ void zface_wws(const Geom &g, const R *__restrict__ face_rho,
                                           int x, int y, int z, R f[Q]) {
   using V = VSet<Q>;
@@ -476,7 +482,8 @@ __device__ __forceinline__ void zface_wws(const Geom &g, const R *__restrict__ f
     if constexpr ((FC == 4 && ez > 0) || (FC == 5 && ez < 0)) {
       const R eu = (R)V::ex(i) * Cst<R>::uw(g, FC, 0) + (R)V::ey(i) * Cst<R>::uw(g, FC, 1) +
                    (R)ez * Cst<R>::uw(g, FC, 2);
-      f[i] = f[i] - R(2) * (rho_t * V::template wr<R>(i)) * eu * Cst<R>::inv_cs2(g);
+      constexpr R w = V::template wr<R>(i) * R(1 << SH);   // working units
+      f[i] = f[i] - R(2) * (rho_t * w) * eu * Cst<R>::inv_cs2(g);
     }
   });
 }
@@ -508,8 +515,9 @@ __device__ __forceinline__ void pull_row_node(const StepPlanes &p, const Geom &g
     else
       f[i] = St::load(src, V::template wr<typename St::R>(i));
   });
-  if (bottom && g.face[4] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 4>(g, face_rho, x, y, z, f);
-  if (top && g.face[5] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 5>(g, face_rho, x, y, z, f);
+  constexpr int kSh = WORK ? St::kShift : 0;
+  if (bottom && g.face[4] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 4, kSh>(g, face_rho, x, y, z, f);
+  if (top && g.face[5] == LBM_BC_WALL_WITH_SPEED) zface_wws<Q, 5, kSh>(g, face_rho, x, y, z, f);
 }
 
 // Rolled value (periodic wrap on every axis, no face rule): what the
@@ -592,7 +600,7 @@ __device__ __forceinline__ R edot(R vx, R vy, R vz) {
 //   f_i += (1 - 1/(2 tau)) w_i [ (e_i - u)/cs^2 + (u o e_i) o e_i / cs^4 ] . F
 // (component-wise u_k e_ik^2, the reference's form).  For the pair (i, j),
 // e_j = -e_i: the e.F part flips sign, the rest is shared.
-template <int Q, typename R>
+template <int Q, int SH = 0, typename R>
 __device__ __forceinline__ void add_force(R f[Q], const Geom &g, R ux, R uy, R uz, R fx, R fy,
                                           R fz) {
   using V = VSet<Q>;
@@ -603,7 +611,7 @@ __device__ __forceinline__ void add_force(R f[Q], const Geom &g, R ux, R uy, R u
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     constexpr int j = V::rev(i);
-    constexpr R cw = V::template wr<R>(i);
+    constexpr R cw = V::template wr<R>(i) * R(1 << SH);     // working units
     if constexpr (i == 0) {
       f[0] = LBM_FMA(force_c * cw, base, f[0]);
     } else if constexpr (i < j) {
@@ -667,7 +675,7 @@ __device__ __forceinline__ void collide(R f[Q], const Geom &g, R rho, R ux, R uy
 // so the pair (i, rev(i)) gets A +- B with
 //   A = w (drho - rho |u|^2/(2cs^2)) / tau + (w rho t / (2 tau)) t,  B = w rho t / tau.
 // The forcing term (add_force) is additive and applies to d unchanged.
-template <int Q>
+template <int Q, int SH = 0>
 __device__ __forceinline__ void dev_moments(const float d[Q], float fx, float fy, float fz,
                                             bool face, float &rho, float &drho, float &ux,
                                             float &uy, float &uz) {
@@ -688,15 +696,16 @@ __device__ __forceinline__ void dev_moments(const float d[Q], float fx, float fy
       if constexpr (V::ez(i) < 0) jz -= t;
     }
   });
-  drho = r;
-  rho = 1.f + r;
+  constexpr float kUnscale = 1.f / (float)(1 << SH);      // d = working value / 2^SH
+  drho = r * kUnscale;
+  rho = 1.f + drho;
   const float inv = 1.f / rho;
-  ux = face ? 0.f : LBM_FMA(0.5f, fx, jx) * inv;
-  uy = face ? 0.f : LBM_FMA(0.5f, fy, jy) * inv;
-  uz = face ? 0.f : LBM_FMA(0.5f, fz, jz) * inv;
+  ux = face ? 0.f : LBM_FMA(0.5f, fx, jx * kUnscale) * inv;
+  uy = face ? 0.f : LBM_FMA(0.5f, fy, jy * kUnscale) * inv;
+  uz = face ? 0.f : LBM_FMA(0.5f, fz, jz * kUnscale) * inv;
 }
 
-template <int Q>
+template <int Q, int SH = 0>
 __device__ __forceinline__ void collide_dev(float d[Q], const Geom &g, float rho, float drho,
                                             float ux, float uy, float uz) {
   using V = VSet<Q>;
@@ -708,7 +717,7 @@ __device__ __forceinline__ void collide_dev(float d[Q], const Geom &g, float rho
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     constexpr int j = V::rev(i);
-    constexpr float w = V::w(i);
+    constexpr float w = V::w(i) * (float)(1 << SH);         // working units
     if constexpr (i == 0) {
       d[0] = LBM_FMA(d[0], keep, w * c);
     } else if constexpr (i < j) {

@@ -75,7 +75,7 @@ __device__ __forceinline__ ChunkForce chunk_force(const StepArgs &a, unsigned id
 
 // finish_node_m also hands the node's end-of-step moments (the second
 // update_u_rou) to the caller.
-template <int Q, bool FORCE, bool DEV, typename R>
+template <int Q, bool FORCE, bool DEV, int SH, typename R>
 __device__ __forceinline__ void finish_node_m(const StepArgs &a, R f[Q], unsigned idx, int x,
                                               int y, int z, bool face, ChunkForce cf,
                                               unsigned &bad, R &rho_out, R &ux_out, R &uy_out,
@@ -97,7 +97,7 @@ __device__ __forceinline__ void finish_node_m(const StepArgs &a, R f[Q], unsigne
   }
   R rho, drho = R(0), ux, uy, uz;
   if constexpr (DEV)
-    dev_moments<Q>(f, fox, foy, foz, face, rho, drho, ux, uy, uz);
+    dev_moments<Q, SH>(f, fox, foy, foz, face, rho, drho, ux, uy, uz);
   else
     moments<Q>(f, fox, foy, foz, face, rho, ux, uy, uz);
   // Where both the previous and this step's force are zero (everywhere
@@ -107,9 +107,9 @@ __device__ __forceinline__ void finish_node_m(const StepArgs &a, R f[Q], unsigne
   // enough: the second pass drops the previous force from u.)
   if (FORCE && (fnx != R(0) || fny != R(0) || fnz != R(0) || fox != R(0) || foy != R(0) ||
                 foz != R(0))) {
-    add_force<Q>(f, a.g, ux, uy, uz, fnx, fny, fnz);
+    add_force<Q, SH>(f, a.g, ux, uy, uz, fnx, fny, fnz);
     if constexpr (DEV)
-      dev_moments<Q>(f, fnx, fny, fnz, face, rho, drho, ux, uy, uz);
+      dev_moments<Q, SH>(f, fnx, fny, fnz, face, rho, drho, ux, uy, uz);
     else
       moments<Q>(f, fnx, fny, fnz, face, rho, ux, uy, uz);
   }
@@ -120,7 +120,8 @@ __device__ __forceinline__ void finish_node_m(const StepArgs &a, R f[Q], unsigne
     R *of = static_cast<R *>(a.obs_f);
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      of[(long long)i * a.g.n + idx] = DEV ? f[i] + V::template wr<R>(i) : f[i];
+      of[(long long)i * a.g.n + idx] =
+          DEV ? f[i] * (R(1) / R(1 << SH)) + V::template wr<R>(i) : f[i];
     });
   }
   if (a.obs_rho != nullptr) static_cast<R *>(a.obs_rho)[idx] = rho;
@@ -136,18 +137,18 @@ __device__ __forceinline__ void finish_node_m(const StepArgs &a, R f[Q], unsigne
   uz_out = uz;
   if (a.fb != nullptr) {
     if constexpr (DEV)
-      collide_dev<Q>(f, a.g, rho, drho, ux, uy, uz);
+      collide_dev<Q, SH>(f, a.g, rho, drho, ux, uy, uz);
     else
       collide<Q>(f, a.g, rho, ux, uy, uz);
   }
 }
 
-template <int Q, bool FORCE, bool DEV, typename R>
+template <int Q, bool FORCE, bool DEV, int SH, typename R>
 __device__ __forceinline__ void finish_node(const StepArgs &a, R f[Q], unsigned idx, int x,
                                             int y, int z, bool face, ChunkForce cf,
                                             unsigned &bad) {
   R rho, ux, uy, uz;
-  finish_node_m<Q, FORCE, DEV>(a, f, idx, x, y, z, face, cf, bad, rho, ux, uy, uz);
+  finish_node_m<Q, FORCE, DEV, SH>(a, f, idx, x, y, z, face, cf, bad, rho, ux, uy, uz);
 }
 
 __device__ __forceinline__ void report_bad(unsigned *status, unsigned bad) {
@@ -217,7 +218,7 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
   else
     pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, face_rho, f);
   unsigned bad = 0;
-  finish_node<Q, FORCE, St::kDev>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1, cf,
+  finish_node<Q, FORCE, St::kDev, St::kShift>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1, cf,
                                   bad);
   report_bad(a.status, bad);
   if (a.fb != nullptr) {
@@ -304,13 +305,13 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const __grid_constant__
     else
       pull_general<Q, S, true>(static_cast<const T *>(a.fa), a.g, x, y, z, face_rho, f);
     R rho, ux, uy, uz;
-    finish_node_m<Q, FORCE, St::kDev>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1,
+    finish_node_m<Q, FORCE, St::kDev, St::kShift>(a, f, idx, x, y, z, !row_in || z == 0 || z == a.g.nz - 1,
                                       cf, bad, rho, ux, uy, uz);
     R fmn = R(INFINITY), fmx = -R(INFINITY);
     double fsum = 0.0;
     static_for<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      const R v = St::kDev ? f[i] + V::template wr<R>(i) : f[i];
+      const R v = St::kDev ? f[i] * (R(1) / R(1 << St::kShift)) + V::template wr<R>(i) : f[i];
       fsum += (double)v;
       fmn = fmin(fmn, v);
       fmx = fmax(fmx, v);
@@ -421,7 +422,7 @@ __device__ __forceinline__ void face_row_nodes(const StepArgs &a, unsigned idx0,
     R f[Q];
     pull_general<Q, S, true>(fa, a.g, x, y, z0 + k, face_rho, f);
     // the nodes may lie in two chunks
-    finish_node<Q, FORCE, St::kDev>(a, f, idx0 + k, x, y, z0 + k, on_any_face(a.g, x, y, z0 + k),
+    finish_node<Q, FORCE, St::kDev, St::kShift>(a, f, idx0 + k, x, y, z0 + k, on_any_face(a.g, x, y, z0 + k),
                                     chunk_force<FORCE>(a, idx0 + k), bad);
     if (a.fb != nullptr) {
       static_for<Q>([&](auto ic) {
@@ -527,9 +528,9 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
         }
       });
       if (pr == 0 && bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
-        zface_wws<Q, 4>(a.g, static_cast<const float *>(a.face_rho_in), x, y, 0, f0);
+        zface_wws<Q, 4, St::kShift>(a.g, static_cast<const float *>(a.face_rho_in), x, y, 0, f0);
       if (pr == kWords - 1 && top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
-        zface_wws<Q, 5>(a.g, static_cast<const float *>(a.face_rho_in), x, y, a.g.nz - 1, f1);
+        zface_wws<Q, 5, St::kShift>(a.g, static_cast<const float *>(a.face_rho_in), x, y, a.g.nz - 1, f1);
     } else if constexpr (!kCompact) {
       const T *fa = static_cast<const T *>(a.fa);
       const float *face_rho = static_cast<const float *>(a.face_rho_in);
@@ -539,11 +540,11 @@ __device__ __forceinline__ void step_vec_pairs_at(const StepArgs &a, const unsig
     }
     // (a pair may straddle two force chunks: dense rows of any length)
     if (2 * pr < nv)
-      finish_node<Q, FORCE, true>(a, f0, idx0 + 2 * pr, x, y, za,
+      finish_node<Q, FORCE, true, St::kShift>(a, f0, idx0 + 2 * pr, x, y, za,
                                   !row_in || za == 0 || za == a.g.nz - 1,
                                   chunk_force<FORCE>(a, idx0 + 2 * pr), bad);
     if (2 * pr + 1 < nv)
-      finish_node<Q, FORCE, true>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
+      finish_node<Q, FORCE, true, St::kShift>(a, f1, idx0 + 2 * pr + 1, x, y, za + 1,
                                   !row_in || za + 1 == a.g.nz - 1,
                                   chunk_force<FORCE>(a, idx0 + 2 * pr + 1), bad);
     if (a.fb != nullptr) {
@@ -660,9 +661,9 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
       }
     });
     if (bottom && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
-      zface_wws<Q, 4>(a.g, face_rho, x, y, 0, f[0]);
+      zface_wws<Q, 4, St::kShift>(a.g, face_rho, x, y, 0, f[0]);
     if (top && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
-      zface_wws<Q, 5>(a.g, face_rho, x, y, a.g.nz - 1, f[NZ - 1]);
+      zface_wws<Q, 5, St::kShift>(a.g, face_rho, x, y, a.g.nz - 1, f[NZ - 1]);
   } else if constexpr (!kCompact) {
     const T *fa = static_cast<const T *>(a.fa);
     // (padding lanes repeat the row's last node; they are not finished)
@@ -677,7 +678,7 @@ __device__ __forceinline__ void step_vec_body(const StepArgs &a, const unsigned 
     const int z = z0 + k;
     // (a thread's nodes may straddle two force chunks: dense rows of any length)
     if (k < nv)
-      finish_node<Q, FORCE, St::kDev>(a, f[k], idx0 + k, x, y, z,
+      finish_node<Q, FORCE, St::kDev, St::kShift>(a, f[k], idx0 + k, x, y, z,
                                       !row_in || z == 0 || z == a.g.nz - 1,
                                       chunk_force<FORCE>(a, idx0 + k), bad);
   }
@@ -830,7 +831,7 @@ __device__ __forceinline__ float sm_elem(const typename Storage<S>::T *p) {
   if constexpr (Storage<S>::kBits == 32)
     return *p;
   else if constexpr (S == LBM_STORAGE_FP16S)
-    return Storage<S>::cvt(*p);
+    return __half2float(*p);
   else
     return __bfloat162float(*p);
 }
@@ -945,16 +946,16 @@ __global__ void __launch_bounds__(kTmaThreads) k_step_tma(const __grid_constant_
           }
         });
         if (z == 0 && a.g.face[4] == LBM_BC_WALL_WITH_SPEED)
-          zface_wws<Q, 4>(a.g, face_rho, x, y, 0, f0);
+          zface_wws<Q, 4, St::kShift>(a.g, face_rho, x, y, 0, f0);
         if (z + 2 == nz && a.g.face[5] == LBM_BC_WALL_WITH_SPEED)
-          zface_wws<Q, 5>(a.g, face_rho, x, y, nz - 1, f1);
+          zface_wws<Q, 5, St::kShift>(a.g, face_rho, x, y, nz - 1, f1);
       } else {
         pull_general<Q, S, true>(fa, a.g, x, y, z, face_rho, f0);
         pull_general<Q, S, true>(fa, a.g, x, y, z + 1, face_rho, f1);
       }
       unsigned bad = 0;
-      finish_node<Q, FORCE, St::kDev>(a, f0, idx, x, y, z, !row_in || z == 0, cf, bad);
-      finish_node<Q, FORCE, St::kDev>(a, f1, idx + 1, x, y, z + 1, !row_in || z + 1 == nz - 1, cf,
+      finish_node<Q, FORCE, St::kDev, St::kShift>(a, f0, idx, x, y, z, !row_in || z == 0, cf, bad);
+      finish_node<Q, FORCE, St::kDev, St::kShift>(a, f1, idx + 1, x, y, z + 1, !row_in || z + 1 == nz - 1, cf,
                                       bad);
       report_bad(a.status, bad);
       if (a.fb != nullptr) {
