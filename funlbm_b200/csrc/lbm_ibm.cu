@@ -11,7 +11,7 @@ namespace lbm {
 constexpr int kStencil = 64;                // 4 x 4 x 4 nodes per marker
 constexpr int kMarkersPerBlock = 4;         // interpolation / spreading blocks
 constexpr int kIbmThreads = kStencil * kMarkersPerBlock;
-constexpr int kRigidThreads = 256;
+constexpr int kRigidThreads = 512;
 
 // Stencil box of lbm/lbm3d.py:32-44 for marker position `l` on one axis:
 // lo = max(floor(l) - 1, 0), hi = min(lo + 4, size) with size = nodes - 1
@@ -265,6 +265,80 @@ __device__ __forceinline__ void argext_merge(R &v, int &i, R v2, int i2, bool wa
   }
 }
 
+// Newton-Euler update of particle pi (update_from_lar, particle/base/
+// base.py:120-152), one block: a single pass over the markers gives the
+// float64 sums A = sum lF lm and B = sum (lx x lF) lm, then thread 0 writes
+// cF = -A + (1 - rho_p / rho_f) mass [gl, 0, 0], cu, cx, and the torque about
+// the new centre, cT = -(B - cx x A): the reference's -sum((lx - cx) x lF lm)
+// with the centre taken out of the sum, so the torque needs no second pass
+// after cx is known.  With s_ang set, also angle += cw (particle/coord.py:
+// 107).  Returns with s_cx (and s_ang) filled for every thread.
+template <typename R>
+__device__ __forceinline__ void rigid_update_block(const RigidArgs &a, const PView<R> &P, int pi,
+                                                   int m0, int m1,
+                                                   double (*s_sum)[kRigidThreads / 32], R *s_cx,
+                                                   R *s_ang) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double sm[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    const double lm = P.lm[m];
+    const double fx = (double)P.lF[3 * m] * lm, fy = (double)P.lF[3 * m + 1] * lm,
+                 fz = (double)P.lF[3 * m + 2] * lm;
+    const double x = P.lx[3 * m], y = P.lx[3 * m + 1], z = P.lx[3 * m + 2];
+    sm[0] += fx;
+    sm[1] += fy;
+    sm[2] += fz;
+    sm[3] += y * fz - z * fy;
+    sm[4] += z * fx - x * fz;
+    sm[5] += x * fy - y * fx;
+  }
+  for (int k = 0; k < 6; ++k) {
+    for (int o = 16; o > 0; o >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], o);
+    if (lane == 0) s_sum[k][wid] = sm[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double A[3], B[3];
+    for (int k = 0; k < 3; ++k) {
+      A[k] = 0.0;
+      B[k] = 0.0;
+      for (int w = 0; w < kRigidThreads / 32; ++w) {
+        A[k] += s_sum[k][w];
+        B[k] += s_sum[k + 3][w];
+      }
+    }
+    const R mass = P.mass[pi];
+    const R buoy = (R)(1.0 - (double)P.rou[pi] / (double)a.rouf) * mass;
+    double c[3];
+    for (int k = 0; k < 3; ++k) {
+      const R cf = (R)(-A[k]) + (k == 0 ? buoy * (R)a.gl : R(0));
+      P.cF[3 * pi + k] = cf;
+      const R cu = P.cu[3 * pi + k] + cf / mass * (R)a.dt;
+      P.cu[3 * pi + k] = cu;
+      const R cx = P.cx[3 * pi + k] + cu * (R)a.dt;
+      P.cx[3 * pi + k] = cx;
+      s_cx[k] = cx;
+      c[k] = (double)cx;
+    }
+    const double T[3] = {B[0] - (c[1] * A[2] - c[2] * A[1]), B[1] - (c[2] * A[0] - c[0] * A[2]),
+                         B[2] - (c[0] * A[1] - c[1] * A[0])};
+    for (int k = 0; k < 3; ++k) {
+      const R ct = -(R)T[k];
+      P.cT[3 * pi + k] = ct;
+      const R cw = P.cw[3 * pi + k] + R(0.1) * ct * (R)a.dt / P.inertia[3 * pi + k];
+      P.cw[3 * pi + k] = cw;
+      if (s_ang != nullptr) {
+        // shared, so that no thread reads the rotation vector after it is
+        // overwritten
+        const R ang = P.angle[3 * pi + k] + cw;
+        s_ang[k] = ang;
+        P.angle[3 * pi + k] = ang;
+      }
+    }
+  }
+  __syncthreads();
+}
+
 template <typename R>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
   const PView<R> P = pview<R>(a.p);
@@ -273,7 +347,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
   __shared__ R s_v[6][kRigidThreads / 32];
   __shared__ int s_i[6][kRigidThreads / 32];
   __shared__ int s_ext[6];
-  __shared__ double s_sum[3][kRigidThreads / 32];
+  __shared__ double s_sum[6][kRigidThreads / 32];
   __shared__ R s_cx[3];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 
@@ -338,62 +412,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
   }
   __syncthreads();
   if (!(a.what & RIGID_UPDATE)) return;
-
-  // -- cF = sum(-lF lm) + (1 - rho_p / rho_f) mass [gl, 0, 0]   (float64 sums)
-  double sf[3] = {0.0, 0.0, 0.0};
-  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double lm = P.lm[m];
-    for (int k = 0; k < 3; ++k) sf[k] += -(double)P.lF[3 * m + k] * lm;
-  }
-  for (int k = 0; k < 3; ++k) {
-    for (int o = 16; o > 0; o >>= 1) sf[k] += __shfl_xor_sync(0xffffffffu, sf[k], o);
-    if (lane == 0) s_sum[k][wid] = sf[k];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const R mass = P.mass[pi];
-    const R buoy = (R)(1.0 - (double)P.rou[pi] / (double)a.rouf) * mass;
-    for (int k = 0; k < 3; ++k) {
-      double t = 0.0;
-      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
-      const R cf = (R)t + (k == 0 ? buoy * (R)a.gl : R(0));
-      P.cF[3 * pi + k] = cf;
-      const R cu = P.cu[3 * pi + k] + cf / mass * (R)a.dt;
-      P.cu[3 * pi + k] = cu;
-      const R cx = P.cx[3 * pi + k] + cu * (R)a.dt;
-      P.cx[3 * pi + k] = cx;
-      s_cx[k] = cx;
-    }
-  }
-  __syncthreads();
-
-  // -- cT = -sum((lx - cx) x lF lm)  with the new cx   (float64 sums)
-  double st[3] = {0.0, 0.0, 0.0};
-  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double rx = (double)(P.lx[3 * m] - s_cx[0]);
-    const double ry = (double)(P.lx[3 * m + 1] - s_cx[1]);
-    const double rz = (double)(P.lx[3 * m + 2] - s_cx[2]);
-    const double fx = P.lF[3 * m], fy = P.lF[3 * m + 1], fz = P.lF[3 * m + 2];
-    const double lm = P.lm[m];
-    st[0] += (ry * fz - rz * fy) * lm;
-    st[1] += (rz * fx - rx * fz) * lm;
-    st[2] += (rx * fy - ry * fx) * lm;
-  }
-  __syncthreads();
-  for (int k = 0; k < 3; ++k) {
-    for (int o = 16; o > 0; o >>= 1) st[k] += __shfl_xor_sync(0xffffffffu, st[k], o);
-    if (lane == 0) s_sum[k][wid] = st[k];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < 3; ++k) {
-      double t = 0.0;
-      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
-      const R ct = -(R)t;
-      P.cT[3 * pi + k] = ct;
-      P.cw[3 * pi + k] = P.cw[3 * pi + k] + R(0.1) * ct * (R)a.dt / P.inertia[3 * pi + k];
-    }
-  }
+  rigid_update_block<R>(a, P, pi, m0, m1, s_sum, s_cx, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -684,25 +703,12 @@ __global__ void __launch_bounds__(kRigidThreads) k_markers(const lbm_particles p
 // the markers LBMD3.particle_to_wall acts on (lbm/lbm3d.py:121-167).
 // Thread 0 receives them in ext.
 // ---------------------------------------------------------------------------
+// Block-wide argmin / argmax (first index on ties) of the per-thread
+// candidates v / id (argmin x, y, z then argmax x, y, z); thread 0 gets ext.
 template <typename R>
-__device__ __forceinline__ void block_extremes(const PView<R> &P, int m0, int m1,
-                                               R (*s_v)[kRigidThreads / 32],
-                                               int (*s_i)[kRigidThreads / 32], int ext[6]) {
+__device__ __forceinline__ void extremes_reduce(R v[6], int id[6], R (*s_v)[kRigidThreads / 32],
+                                                int (*s_i)[kRigidThreads / 32], int ext[6]) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  R v[6];
-  int id[6];
-  for (int k = 0; k < 3; ++k) {
-    v[k] = R(INFINITY);
-    v[k + 3] = -R(INFINITY);
-    id[k] = id[k + 3] = 0x7fffffff;
-  }
-  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    for (int k = 0; k < 3; ++k) {
-      const R c = P.lx[3 * m + k];
-      argext_merge(v[k], id[k], c, m, true);
-      argext_merge(v[k + 3], id[k + 3], c, m, false);
-    }
-  }
   for (int k = 0; k < 6; ++k) {
     for (int o = 16; o > 0; o >>= 1) {
       const R v2 = __shfl_xor_sync(0xffffffffu, v[k], o);
@@ -726,6 +732,28 @@ __device__ __forceinline__ void block_extremes(const PView<R> &P, int m0, int m1
   __syncthreads();
 }
 
+// The six extreme markers of particle markers m0..m1 (one block).
+template <typename R>
+__device__ __forceinline__ void block_extremes(const PView<R> &P, int m0, int m1,
+                                               R (*s_v)[kRigidThreads / 32],
+                                               int (*s_i)[kRigidThreads / 32], int ext[6]) {
+  R v[6];
+  int id[6];
+  for (int k = 0; k < 3; ++k) {
+    v[k] = R(INFINITY);
+    v[k + 3] = -R(INFINITY);
+    id[k] = id[k + 3] = 0x7fffffff;
+  }
+  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
+    for (int k = 0; k < 3; ++k) {
+      const R c = P.lx[3 * m + k];
+      argext_merge(v[k], id[k], c, m, true);
+      argext_merge(v[k + 3], id[k + 3], c, m, false);
+    }
+  }
+  extremes_reduce<R>(v, id, s_v, s_i, ext);
+}
+
 template <typename R>
 __global__ void __launch_bounds__(kRigidThreads) k_extremes(const lbm_particles pt) {
   const PView<R> P = pview<R>(pt);
@@ -739,81 +767,20 @@ __global__ void __launch_bounds__(kRigidThreads) k_extremes(const lbm_particles 
 }
 
 // Rigid update + marker transform + extremes of the new positions, one block
-// per particle: the RIGID_UPDATE part of k_rigid, then k_markers' rotation,
-// with the same arithmetic and summation order (so the same results).
+// per particle: rigid_update_block (as k_rigid's RIGID_UPDATE), then
+// k_markers' rotation with the extreme markers of the new positions found
+// in the same pass -- the same arithmetic and order, so the same results.
 template <typename R>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a) {
   const PView<R> P = pview<R>(a.p);
   const int pi = blockIdx.x;
   const int m0 = P.offset[pi], m1 = P.offset[pi + 1];
-  __shared__ double s_sum[3][kRigidThreads / 32];
+  __shared__ double s_sum[6][kRigidThreads / 32];
   __shared__ R s_cx[3], s_ang[3];
   __shared__ R s_v[6][kRigidThreads / 32];
   __shared__ int s_i[6][kRigidThreads / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-
-  // -- cF = sum(-lF lm) + (1 - rho_p / rho_f) mass [gl, 0, 0]   (float64 sums)
-  double sf[3] = {0.0, 0.0, 0.0};
-  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double lm = P.lm[m];
-    for (int k = 0; k < 3; ++k) sf[k] += -(double)P.lF[3 * m + k] * lm;
-  }
-  for (int k = 0; k < 3; ++k) {
-    for (int o = 16; o > 0; o >>= 1) sf[k] += __shfl_xor_sync(0xffffffffu, sf[k], o);
-    if (lane == 0) s_sum[k][wid] = sf[k];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const R mass = P.mass[pi];
-    const R buoy = (R)(1.0 - (double)P.rou[pi] / (double)a.rouf) * mass;
-    for (int k = 0; k < 3; ++k) {
-      double t = 0.0;
-      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
-      const R cf = (R)t + (k == 0 ? buoy * (R)a.gl : R(0));
-      P.cF[3 * pi + k] = cf;
-      const R cu = P.cu[3 * pi + k] + cf / mass * (R)a.dt;
-      P.cu[3 * pi + k] = cu;
-      const R cx = P.cx[3 * pi + k] + cu * (R)a.dt;
-      P.cx[3 * pi + k] = cx;
-      s_cx[k] = cx;
-    }
-  }
-  __syncthreads();
-
-  // -- cT = -sum((lx - cx) x lF lm)  with the new cx   (float64 sums)
-  double st[3] = {0.0, 0.0, 0.0};
-  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double rx = (double)(P.lx[3 * m] - s_cx[0]);
-    const double ry = (double)(P.lx[3 * m + 1] - s_cx[1]);
-    const double rz = (double)(P.lx[3 * m + 2] - s_cx[2]);
-    const double fx = P.lF[3 * m], fy = P.lF[3 * m + 1], fz = P.lF[3 * m + 2];
-    const double lm = P.lm[m];
-    st[0] += (ry * fz - rz * fy) * lm;
-    st[1] += (rz * fx - rx * fz) * lm;
-    st[2] += (rx * fy - ry * fx) * lm;
-  }
-  __syncthreads();
-  for (int k = 0; k < 3; ++k) {
-    for (int o = 16; o > 0; o >>= 1) st[k] += __shfl_xor_sync(0xffffffffu, st[k], o);
-    if (lane == 0) s_sum[k][wid] = st[k];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < 3; ++k) {
-      double t = 0.0;
-      for (int w = 0; w < kRigidThreads / 32; ++w) t += s_sum[k][w];
-      const R ct = -(R)t;
-      P.cT[3 * pi + k] = ct;
-      const R cw = P.cw[3 * pi + k] + R(0.1) * ct * (R)a.dt / P.inertia[3 * pi + k];
-      P.cw[3 * pi + k] = cw;
-      // angle += cw (particle/coord.py:107), shared so that no thread reads
-      // the rotation vector after it is overwritten
-      const R ang = P.angle[3 * pi + k] + cw;
-      s_ang[k] = ang;
-      P.angle[3 * pi + k] = ang;
-    }
-  }
-  __syncthreads();   // every thread has read lx for the torque; cw and angle are final
+  rigid_update_block<R>(a, P, pi, m0, m1, s_sum, s_cx, s_ang);
+  // (every thread has read lx for the sums; cw and angle are final)
 
   // -- lx = R(angle) X0 + cx   (particle/coord.py:87-108)
   double v[3];
@@ -839,17 +806,27 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
   const double M[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w),     2 * (x * z + y * w),
                        2 * (x * y + z * w),     1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
                        2 * (x * z - y * w),     2 * (y * z + x * w),     1 - 2 * (x * x + y * y)};
+  const bool ext_on = a.p.extreme != nullptr;
+  R ev[6];
+  int eid[6];
+  for (int k = 0; k < 3; ++k) {
+    ev[k] = R(INFINITY);
+    ev[k + 3] = -R(INFINITY);
+    eid[k] = eid[k + 3] = 0x7fffffff;
+  }
   for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
     const double X = P.lagrange[3 * m], Y = P.lagrange[3 * m + 1], Z = P.lagrange[3 * m + 2];
     for (int k = 0; k < 3; ++k) {
       const double r = M[3 * k] * X + M[3 * k + 1] * Y + M[3 * k + 2] * Z;
-      P.lx[3 * m + k] = (R)r + c[k];
+      const R nx = (R)r + c[k];
+      P.lx[3 * m + k] = nx;
+      argext_merge(ev[k], eid[k], nx, m, true);
+      argext_merge(ev[k + 3], eid[k + 3], nx, m, false);
     }
   }
-  if (a.p.extreme == nullptr) return;
-  __syncthreads();   // the new positions are written
+  if (!ext_on) return;
   int ext[6];
-  block_extremes<R>(P, m0, m1, s_v, s_i, ext);
+  extremes_reduce<R>(ev, eid, s_v, s_i, ext);
   if (threadIdx.x == 0)
     for (int k = 0; k < 6; ++k) a.p.extreme[6 * pi + k] = ext[k];
 }
