@@ -232,11 +232,20 @@ __device__ __forceinline__ void step_scalar_body(const StepArgs &a, const unsign
 }
 
 // Register cap of the one-node kernel (resident blocks per SM asked of the
-// compiler, 0 = none): 16-bit D3Q19 at 48 registers (5 blocks of 256; a few
-// spilled words) -- the kernel rows of odd length run in 16-bit storage.
+// compiler, 0 = none).  The one-node kernel runs the rows of odd length (the
+// reference's size + 1 nodes) and is latency-bound there: an ncu capture of
+// the forced D3Q27 FP32 step on 257 x 129 x 129 nodes showed 74 registers,
+// 3 resident blocks of 256 (24 warps / SM) and 7.7 long-scoreboard stalls
+// per issue.  D3Q19 in FP32 and 16-bit storage: 48 registers (5 blocks; the
+// forced 16-bit kernel spills a few words); D3Q27 in FP32 and 16-bit: 64
+// registers (4 blocks), no spills.
 template <int Q, int S>
 constexpr int scalar_min_blocks() {
-  return (Storage<S>::kBits == 16 && Q == 19) ? 5 : 0;
+  constexpr int bits = Storage<S>::kBits;
+  if (bits == 64) return 0;
+  if (Q == 19) return 5;
+  if (Q == 27) return 4;
+  return 0;
 }
 
 template <int Q, int S, bool FORCE>
