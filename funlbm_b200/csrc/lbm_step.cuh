@@ -1138,15 +1138,18 @@ struct StepLauncher {
     if (nodes == LBM_STEP_ROWS) return go_tma(a, force, s);
     const bool odd_pairs = bits == 16 && a.g.pz % 2 == 1 && a.g.nz >= 3;
     if (nodes == 0) {
-      // Measured on B200 (D3Q19): node pairs with 128-thread blocks are the
-      // fastest shape wherever rows allow them -- 512^3 FP32 3027 us (one
-      // node per thread 3066 us; 3035 against 3132 us over seconds under
-      // the power cap, where the pair kernel holds 1935 MHz and the other
-      // 1845), 512^3 fp16s 1869 us (4 nodes 1985 us).  Rows of odd length
-      // without pitch take one node per thread (on the walled 161x65x65 and
+      // Measured on B200 at 512^3: node pairs with 128-thread blocks are the
+      // fastest shape wherever rows allow them (D3Q19 FP32 3027 us, one node
+      // per thread 3045 us; 3035 against 3132 us over seconds under the
+      // power cap, where the pair kernel holds 1935 MHz and the other 1845),
+      // except unforced D3Q13 / D3Q19 in 16-bit storage, where 4 nodes per
+      // thread are (D3Q19 fp16s 1818 against 1881 us, bf16s 2075 against
+      // 2325; D3Q13 fp16s 1594 against 1768).  Rows of odd length without
+      // pitch take one node per thread (on the walled 161x65x65 and
       // 257x129x129 lattices also faster than pitched pairs); the odd-row
       // pair kernel is a tuner candidate only.
-      nodes = step_shape_ok(2, a.g.pz, bits) ? 2 : 1;
+      const int want = (bits == 16 && (Q == 13 || Q == 19) && !force) ? 4 : 2;
+      nodes = step_shape_ok(want, a.g.pz, bits) ? want : step_shape_ok(2, a.g.pz, bits) ? 2 : 1;
       threads = threads ? threads : 128;
     }
     if (nodes == 2 && odd_pairs) {

@@ -42,10 +42,14 @@ def shape_ok(nodes, pz, bits, nz=None):
 
 def default_shape(q, storage, pz, forced=False):
     """The launch shape lbm_flow_step uses when none is set (measured best on
-    B200 at 512^3 in FP32 and fp16s): node pairs with 128 threads where the
-    rows allow them, else one node per thread."""
-    if pz % 2 == 0 and pz >= 4:
-        return (2, 128)
+    B200 at 512^3): node pairs with 128 threads where the rows allow them, 4
+    nodes per thread for unforced D3Q13 / D3Q19 in 16-bit storage, else one
+    node per thread."""
+    bits = STORAGE_BITS[storage]
+    want = 4 if (bits == 16 and q in (13, 19) and not forced) else 2
+    for nodes in (want, 2):
+        if pz % nodes == 0 and pz >= 2 * nodes:
+            return (nodes, 128)
     return (1, 256)
 
 

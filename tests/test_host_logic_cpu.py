@@ -76,7 +76,7 @@ def test_added_config_keys():
 
 def test_tuner_keeps_the_default_within_its_margin():
     assert tune.default_shape(19, "fp32", 512) == (2, 128)
-    assert tune.default_shape(19, "fp16s", 512) == (2, 128)
+    assert tune.default_shape(19, "fp16s", 512) == (4, 128)
     assert tune.default_shape(19, "fp16s", 512, forced=True) == (2, 128)
     assert tune.default_shape(27, "bf16s", 514) == (2, 128)
     assert tune.default_shape(19, "fp32", 65) == (1, 256)
