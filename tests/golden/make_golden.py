@@ -21,7 +21,7 @@ Outputs (small float32 ``.npz`` files next to this script):
 
 * ``kat_q{13,15,19,27}.npz``: one call each of ``cul_equ``, ``f_stream``,
   ``update_u_rou`` and ``cul_equ2`` on random states and random face mixes;
-* ``steps_q{19,27}.npz``: ``LBMD3.run_step`` sequences without particles;
+* ``steps_q{13,15,19,27}.npz``: ``LBMD3.run_step`` sequences without particles;
 * ``particles.npz``: ``LBMD3.run_step`` sequences with a sphere and an
   ellipsoid, per-step particle state and flow moments;
 * ``markers.npz``: reference marker sets for the sphere / ellipsoid shapes used
@@ -315,6 +315,11 @@ def main():
                 np.savez_compressed(os.path.join(args.out, "steps_q%d.npz" % q), **make_steps(q, rng))
             np.savez_compressed(os.path.join(args.out, "particles.npz"), **make_particles())
             np.savez_compressed(os.path.join(args.out, "markers.npz"), **make_markers())
+            # D3Q13 / D3Q15 step sequences, from a generator of their own (the
+            # files above keep their random states)
+            rng13 = np.random.default_rng(20261204)
+            for q in (13, 15):
+                np.savez_compressed(os.path.join(args.out, "steps_q%d.npz" % q), **make_steps(q, rng13))
         finally:
             os.chdir(cwd)
 

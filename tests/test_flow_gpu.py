@@ -79,7 +79,7 @@ def _check_state(lbm, ref_f, ref_u, ref_rou):
     assert np.abs(u - ref_u).max() <= 1e-5 * np.abs(ref_u).max() + 2e-7
 
 
-@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("q", [13, 15, 19, 27])
 @pytest.mark.parametrize("fused", [True, False])
 def test_run_step_vs_reference(q, fused):
     """LBMD3.run_step sequences recorded from the reference (12 steps,

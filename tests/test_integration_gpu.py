@@ -71,7 +71,7 @@ print(json.dumps(res))
 """
 
 
-@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("q", [13, 15, 19, 27])
 def test_reference_driver_with_gpu_flow(q, tmp_path):
     require_cuda()
     r = subprocess.run([sys.executable, "-c", CHILD, ROOT, REF, STUBS, str(q), str(tmp_path)],

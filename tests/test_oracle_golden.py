@@ -52,7 +52,7 @@ def test_kat_per_function(q, golden_dir):
         assert _rel(fl.f, g[p + "force_f"]) < 1e-6
 
 
-@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("q", [13, 15, 19, 27])
 def test_run_step_sequences(q, golden_dir):
     """LBMD3.run_step without particles, 12 steps, random PERIODICAL/WALL mixes."""
     g = np.load(os.path.join(golden_dir, "steps_q%d.npz" % q))
