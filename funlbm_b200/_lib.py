@@ -123,6 +123,9 @@ SIGNATURES = {
     "ibm_spread_noalloc": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P]),
     "rigid_update_markers": (I, [_PART, _P]),
     "ibm_interpolate_wall": (I, [_LAT, _P, _FORCE, _P, _PART, F, F, ctypes.c_int32, _P, _P]),
+    "ibm_interpolate_wall_claim": (I, [_LAT, _P, _FORCE, _P, _PART, F, F, ctypes.c_int32, _P,
+                                       _P, _P, _P, _P]),
+    "ibm_spread_claimed": (I, [_LAT, _PART, _P, _P, _P, _P]),
     "rigid_step": (I, [_PART, F, F, F, _P]),
     "ibm_spread_tiled_scratch_bytes": (ctypes.c_size_t, [_LAT, ctypes.c_int32]),
     "ibm_spread_tiled": (I, [_LAT, _PART, ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),

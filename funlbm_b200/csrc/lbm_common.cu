@@ -5,6 +5,7 @@
 #include <vector>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "lbm_api.cuh"
@@ -36,6 +37,14 @@ void set_error(const char *fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
   va_end(ap);
+}
+
+bool chained_launches() {
+  static const bool on = [] {
+    const char *v = std::getenv("FUNLBM_B200_CHAIN");
+    return v == nullptr || std::strcmp(v, "0") != 0;
+  }();
+  return on;
 }
 
 int fail_cuda(cudaError_t e, const char *where) {

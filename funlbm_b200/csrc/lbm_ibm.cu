@@ -128,6 +128,15 @@ struct InterpArgs {
   int wall;            // apply the wall spring at the extreme markers
   float size[3];       // wall positions: nodes - 1 per axis
   float dx;
+  // The first half of reference-mode spreading, fused in (ibm_interpolate_
+  // wall_claim; NULL otherwise): every in-box stencil node of every marker is
+  // claimed in claim_owner (largest marker index), and the blocks from
+  // interp_blocks on clear the chunks of clear_field flagged in clear_chunks
+  // (k_spread_clear's work).  interp_blocks: blocks of the interpolation.
+  int32_t *claim_owner;
+  void *clear_field;
+  uint8_t *clear_chunks;
+  unsigned interp_blocks;
 };
 
 // Wall spring of LBMD3.particle_to_wall (lbm/lbm3d.py:121-167) for marker m
@@ -168,9 +177,38 @@ __device__ __forceinline__ void wall_spring(const PView<R> &P, const int32_t *ex
   lf[2] = out[2];
 }
 
+// Clear the chunks of `field` flagged in `chunks` (the chunks written the last
+// time this buffer was used) and reset their flags.  Each lane reads the flag
+// of chunk `chunk`; the warp then clears its flagged chunks together (3 values
+// per lane per chunk), so a mostly flagged small lattice costs no more than a
+// sparse large one.  Called by whole warps.
+template <typename R>
+__device__ __forceinline__ void clear_flagged_chunks(long long chunk, long long n, R *field,
+                                                     uint8_t *chunks) {
+  const long long nchunks = (n + 31) >> 5;
+  const int lane = threadIdx.x & 31;
+  const bool mine = chunk < nchunks && chunks[chunk] != 0;
+  unsigned todo = __ballot_sync(0xffffffffu, mine);
+  const long long base = chunk - lane;   // first chunk of this warp
+  while (todo != 0) {
+    const int j = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const long long first = (base + j) * 32;
+    const long long count = 3 * ((first + 32 < n ? first + 32 : n) - first);
+    for (long long k = lane; k < count; k += 32) field[3 * first + k] = R(0);
+  }
+  if (mine) chunks[chunk] = 0;
+}
+
 template <int Q, int S>
 __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
+  chain_enter();
   using R = typename Storage<S>::R;
+  if (blockIdx.x >= a.interp_blocks) {   // (the grid has such blocks only with clear_chunks)
+    clear_flagged_chunks<R>((long long)(blockIdx.x - a.interp_blocks) * blockDim.x + threadIdx.x,
+                            a.g.n, static_cast<R *>(a.clear_field), a.clear_chunks);
+    return;
+  }
   __shared__ R sh[3][kMarkersPerBlock * 2];
   const PView<R> P = pview<R>(a.p);
   const int mk = threadIdx.x / kStencil, slot = threadIdx.x % kStencil;
@@ -185,12 +223,16 @@ __global__ void __launch_bounds__(kIbmThreads) k_interp(const InterpArgs a) {
     int x, y, z;
     R w;
     if (stencil_slot(a.g, l, slot, x, y, z, w)) {
+      bool node_ok = true;
       if (!lbm_in(x >= 0 && x < a.g.nx && y >= 0 && y < a.g.ny && z >= 0 && z < a.g.nz)) {
         x = 0;
         y = 0;
         z = 0;
+        node_ok = false;
       }
       const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
+      // (the claim of spreading's pass 0, on the same positions)
+      if (a.claim_owner != nullptr && node_ok) atomicMax(a.claim_owner + idx, m);
       R rho, ux, uy, uz;
       if (a.fa != nullptr) {
         const typename Storage<S>::T *fa = static_cast<const typename Storage<S>::T *>(a.fa);
@@ -280,6 +322,9 @@ __device__ __forceinline__ void rigid_update_block(const RigidArgs &a, const PVi
                                                    R *s_ang) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double sm[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // (unrolled so that the loads of several markers are in flight together;
+  // the sums keep their marker order)
+#pragma unroll 4
   for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
     const double lm = P.lm[m];
     const double fx = (double)P.lF[3 * m] * lm, fy = (double)P.lF[3 * m + 1] * lm,
@@ -424,20 +469,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(const RigidArgs a) {
 // more than a sparse large one.
 template <typename R>
 __global__ void k_spread_clear(long long n, R *field, uint8_t *chunks) {
-  const long long chunk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nchunks = (n + 31) >> 5;
-  const int lane = threadIdx.x & 31;
-  const bool mine = chunk < nchunks && chunks[chunk] != 0;
-  unsigned todo = __ballot_sync(0xffffffffu, mine);
-  const long long base = chunk - lane;   // first chunk of this warp
-  while (todo != 0) {
-    const int j = __ffs(todo) - 1;
-    todo &= todo - 1;
-    const long long first = (base + j) * 32;
-    const long long count = 3 * ((first + 32 < n ? first + 32 : n) - first);
-    for (long long k = lane; k < count; k += 32) field[3 * first + k] = R(0);
-  }
-  if (mine) chunks[chunk] = 0;
+  chain_enter();
+  clear_flagged_chunks<R>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, field, chunks);
 }
 
 struct SpreadArgs {
@@ -452,8 +485,12 @@ struct SpreadArgs {
 // pass 1: the owning marker writes w lF lm (reference mode)
 // pass 2: release the claims
 // pass 3: accumulate w lF lm (accumulate mode; flags set as in pass 0)
+// pass 4: pass 1 after claims made by ibm_interpolate_wall_claim -- the owner
+//         also flags the chunk (every claimed node has exactly one owner, so
+//         the flagged chunks are pass 0's)
 template <int PASS, typename R>
 __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
+  chain_enter();
   __shared__ R sh[1][kMarkersPerBlock * 2];
   const PView<R> P = pview<R>(a.p);
   R *field = static_cast<R *>(a.field);
@@ -488,8 +525,9 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
   if (!in_box) return;
   const R wn = W[0] > R(0) ? w / W[0] : w;
   const R lm = P.lm[m];
-  if (PASS == 1) {
+  if (PASS == 1 || PASS == 4) {
     if (a.owner[idx] != m) return;
+    if (PASS == 4) a.chunks[idx >> 5] = 1;
     for (int k = 0; k < 3; ++k) field[3 * idx + k] = (wn * P.lF[3 * m + k]) * lm;
   } else {
     a.chunks[idx >> 5] = 1;
@@ -772,6 +810,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_extremes(const lbm_particles 
 // in the same pass -- the same arithmetic and order, so the same results.
 template <typename R>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a) {
+  chain_enter();
   const PView<R> P = pview<R>(a.p);
   const int pi = blockIdx.x;
   const int m0 = P.offset[pi], m1 = P.offset[pi + 1];
@@ -779,6 +818,15 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
   __shared__ R s_cx[3], s_ang[3];
   __shared__ R s_v[6][kRigidThreads / 32];
   __shared__ int s_i[6][kRigidThreads / 32];
+  // the body-frame coordinates of this thread's first marker are loaded
+  // before the update, so their latency overlaps it (nothing writes them)
+  int m = m0 + (int)threadIdx.x;
+  double X = 0.0, Y = 0.0, Z = 0.0;
+  if (m < m1) {
+    X = P.lagrange[3 * m];
+    Y = P.lagrange[3 * m + 1];
+    Z = P.lagrange[3 * m + 2];
+  }
   rigid_update_block<R>(a, P, pi, m0, m1, s_sum, s_cx, s_ang);
   // (every thread has read lx for the sums; cw and angle are final)
 
@@ -814,8 +862,15 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
     ev[k + 3] = -R(INFINITY);
     eid[k] = eid[k + 3] = 0x7fffffff;
   }
-  for (int m = m0 + threadIdx.x; m < m1; m += kRigidThreads) {
-    const double X = P.lagrange[3 * m], Y = P.lagrange[3 * m + 1], Z = P.lagrange[3 * m + 2];
+  for (; m < m1; m += kRigidThreads) {
+    // the next marker's coordinates are loaded before this one's stores
+    const int mn = m + kRigidThreads;
+    double Xn = 0.0, Yn = 0.0, Zn = 0.0;
+    if (mn < m1) {
+      Xn = P.lagrange[3 * mn];
+      Yn = P.lagrange[3 * mn + 1];
+      Zn = P.lagrange[3 * mn + 2];
+    }
     for (int k = 0; k < 3; ++k) {
       const double r = M[3 * k] * X + M[3 * k + 1] * Y + M[3 * k + 2] * Z;
       const R nx = (R)r + c[k];
@@ -823,6 +878,9 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
       argext_merge(ev[k], eid[k], nx, m, true);
       argext_merge(ev[k + 3], eid[k + 3], nx, m, false);
     }
+    X = Xn;
+    Y = Yn;
+    Z = Zn;
   }
   if (!ext_on) return;
   int ext[6];
@@ -833,13 +891,17 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_step(const RigidArgs a)
 
 template <int Q>
 struct RunInterp {
-  static int run(const InterpArgs &a, int storage, cudaStream_t s) {
+  static int run(InterpArgs a, int storage, cudaStream_t s) {
     const unsigned nb = (unsigned)((a.p.n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
+    a.interp_blocks = nb;
+    // (clearing blocks after the interpolation's: one thread per 32-node chunk)
+    const unsigned grid =
+        nb + (a.clear_chunks != nullptr ? blocks_for((a.g.n + 31) >> 5, kIbmThreads) : 0u);
     switch (storage) {
-      case LBM_STORAGE_FP32: k_interp<Q, LBM_STORAGE_FP32><<<nb, kIbmThreads, 0, s>>>(a); break;
-      case LBM_STORAGE_FP16S: k_interp<Q, LBM_STORAGE_FP16S><<<nb, kIbmThreads, 0, s>>>(a); break;
-      case LBM_STORAGE_FP64: k_interp<Q, LBM_STORAGE_FP64><<<nb, kIbmThreads, 0, s>>>(a); break;
-      default: k_interp<Q, LBM_STORAGE_BF16S><<<nb, kIbmThreads, 0, s>>>(a); break;
+      case LBM_STORAGE_FP32: launch_chained(k_interp<Q, LBM_STORAGE_FP32>, grid, kIbmThreads, 0, s, a); break;
+      case LBM_STORAGE_FP16S: launch_chained(k_interp<Q, LBM_STORAGE_FP16S>, grid, kIbmThreads, 0, s, a); break;
+      case LBM_STORAGE_FP64: launch_chained(k_interp<Q, LBM_STORAGE_FP64>, grid, kIbmThreads, 0, s, a); break;
+      default: launch_chained(k_interp<Q, LBM_STORAGE_BF16S>, grid, kIbmThreads, 0, s, a); break;
     }
     LBM_LAUNCH_CHECK("ibm_interpolate");
     return LBM_OK;
@@ -871,17 +933,17 @@ template <typename R>
 static int spread_launch(const SpreadArgs &a, int mode, long long n_markers, cudaStream_t s,
                          const char *who) {
   const long long nchunks = (a.g.n + 31) >> 5;
-  k_spread_clear<R><<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, static_cast<R *>(a.field),
+  launch_chained(k_spread_clear<R>, blocks_for(nchunks, 256), 256, 0, s, a.g.n, static_cast<R *>(a.field),
                                                              a.chunks);
   LBM_LAUNCH_CHECK(who);
   if (n_markers == 0) return LBM_OK;
   const unsigned nb = (unsigned)((n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
   if (mode == 0) {
-    k_spread<0, R><<<nb, kIbmThreads, 0, s>>>(a);
-    k_spread<1, R><<<nb, kIbmThreads, 0, s>>>(a);
-    k_spread<2, R><<<nb, kIbmThreads, 0, s>>>(a);
+    launch_chained(k_spread<0, R>, nb, kIbmThreads, 0, s, a);
+    launch_chained(k_spread<1, R>, nb, kIbmThreads, 0, s, a);
+    launch_chained(k_spread<2, R>, nb, kIbmThreads, 0, s, a);
   } else {
-    k_spread<3, R><<<nb, kIbmThreads, 0, s>>>(a);
+    launch_chained(k_spread<3, R>, nb, kIbmThreads, 0, s, a);
   }
   LBM_LAUNCH_CHECK(who);
   return LBM_OK;
@@ -1062,32 +1124,55 @@ int ibm_spread(const lbm_lattice *lat, const lbm_particles *pt, int32_t mode, fl
              : spread_launch<float>(a, mode, pt->n_markers, s, "ibm_spread");
 }
 
-int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force *force,
-                         const float *face_rho_in, const lbm_particles *pt, float dt, float dx,
-                         int32_t step, uint32_t *status, void *stream) {
+}  // extern "C"
+
+namespace lbm {
+// ibm_interpolate_wall, and with field / chunks / owner set
+// ibm_interpolate_wall_claim (the claims and the chunk clearing of reference-
+// mode spreading in the same launch).
+static int interp_wall(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                       const float *face_rho_in, const lbm_particles *pt, float dt, float dx,
+                       int32_t step, uint32_t *status, float *field, uint8_t *chunks,
+                       int32_t *owner, void *stream, const char *who) {
   int rc = check_lattice(lat);
   if (rc) return rc;
-  if ((rc = check_particles(pt, "ibm_interpolate_wall"))) return rc;
+  if ((rc = check_particles(pt, who))) return rc;
   if (!(dt > 0.f)) {
-    set_error("ibm_interpolate_wall: dt must be positive");
+    set_error("%s: dt must be positive", who);
     return LBM_ERR_INVALID;
   }
   if (fa == nullptr) {
-    set_error("ibm_interpolate_wall: needs the post-collision populations");
+    set_error("%s: needs the post-collision populations", who);
     return LBM_ERR_INVALID;
   }
   if (any_face(lat, LBM_BC_NON_EQUILIBRIUM)) {
-    set_error("ibm_interpolate_wall: NON_EQUILIBRIUM faces need the u / rho fields");
+    set_error("%s: NON_EQUILIBRIUM faces need the u / rho fields", who);
     return LBM_ERR_UNSUPPORTED;
   }
   if (any_face(lat, LBM_BC_WALL_WITH_SPEED) && face_rho_in == nullptr) {
-    set_error("ibm_interpolate_wall: WALL_WITH_SPEED faces need face_rho_in");
+    set_error("%s: WALL_WITH_SPEED faces need face_rho_in", who);
     return LBM_ERR_INVALID;
   }
-  if ((rc = check_precision(lat, pt, "ibm_interpolate_wall"))) return rc;
-  if (pt->n_markers == 0) return LBM_OK;
+  const bool claim = chunks != nullptr;
+  if (claim && (field == nullptr || owner == nullptr)) {
+    set_error("%s: field, chunks and owner are required", who);
+    return LBM_ERR_INVALID;
+  }
+  if ((rc = check_precision(lat, pt, who))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (pt->n_markers == 0) {
+    if (!claim) return LBM_OK;
+    // nothing to interpolate or claim: only the clearing
+    const unsigned nb = blocks_for((make_geom(lat).n + 31) >> 5, 256);
+    if (lat->storage == LBM_STORAGE_FP64)
+      launch_chained(k_spread_clear<double>, nb, 256, 0, s, make_geom(lat).n, (double *)field, chunks);
+    else
+      launch_chained(k_spread_clear<float>, nb, 256, 0, s, make_geom(lat).n, field, chunks);
+    LBM_LAUNCH_CHECK(who);
+    return LBM_OK;
+  }
   if (pt->extreme == nullptr) {
-    set_error("ibm_interpolate_wall: the particles' extreme markers are required");
+    set_error("%s: the particles' extreme markers are required", who);
     return LBM_ERR_INVALID;
   }
   InterpArgs a;
@@ -1109,12 +1194,69 @@ int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force
   a.size[1] = (float)(lat->ny - 1);
   a.size[2] = (float)(lat->nz - 1);
   a.dx = dx;
-  switch (lat->q) {
-    case 13: return RunInterp<13>::run(a, lat->storage, (cudaStream_t)stream);
-    case 15: return RunInterp<15>::run(a, lat->storage, (cudaStream_t)stream);
-    case 19: return RunInterp<19>::run(a, lat->storage, (cudaStream_t)stream);
-    default: return RunInterp<27>::run(a, lat->storage, (cudaStream_t)stream);
+  if (claim) {
+    a.claim_owner = owner;
+    a.clear_field = field;
+    a.clear_chunks = chunks;
   }
+  switch (lat->q) {
+    case 13: return RunInterp<13>::run(a, lat->storage, s);
+    case 15: return RunInterp<15>::run(a, lat->storage, s);
+    case 19: return RunInterp<19>::run(a, lat->storage, s);
+    default: return RunInterp<27>::run(a, lat->storage, s);
+  }
+}
+}  // namespace lbm
+
+extern "C" {
+
+int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                         const float *face_rho_in, const lbm_particles *pt, float dt, float dx,
+                         int32_t step, uint32_t *status, void *stream) {
+  return interp_wall(lat, fa, force, face_rho_in, pt, dt, dx, step, status, nullptr, nullptr,
+                     nullptr, stream, "ibm_interpolate_wall");
+}
+
+int ibm_interpolate_wall_claim(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                               const float *face_rho_in, const lbm_particles *pt, float dt,
+                               float dx, int32_t step, uint32_t *status, float *field,
+                               uint8_t *chunks, int32_t *owner, void *stream) {
+  if (chunks == nullptr) {
+    set_error("ibm_interpolate_wall_claim: field, chunks and owner are required");
+    return LBM_ERR_INVALID;
+  }
+  return interp_wall(lat, fa, force, face_rho_in, pt, dt, dx, step, status, field, chunks, owner,
+                     stream, "ibm_interpolate_wall_claim");
+}
+
+int ibm_spread_claimed(const lbm_lattice *lat, const lbm_particles *pt, float *field,
+                       uint8_t *chunks, int32_t *owner, void *stream) {
+  int rc = check_lattice(lat);
+  if (rc) return rc;
+  if ((rc = check_particles(pt, "ibm_spread_claimed"))) return rc;
+  if (field == nullptr || chunks == nullptr || owner == nullptr) {
+    set_error("ibm_spread_claimed: field, chunks and owner are required");
+    return LBM_ERR_INVALID;
+  }
+  if ((rc = check_precision(lat, pt, "ibm_spread_claimed"))) return rc;
+  if (pt->n_markers == 0) return LBM_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  SpreadArgs a;
+  a.g = make_geom(lat);
+  a.p = *pt;
+  a.field = field;
+  a.chunks = chunks;
+  a.owner = owner;
+  const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
+  if (lat->storage == LBM_STORAGE_FP64) {
+    launch_chained(k_spread<4, double>, nb, kIbmThreads, 0, s, a);
+    launch_chained(k_spread<2, double>, nb, kIbmThreads, 0, s, a);
+  } else {
+    launch_chained(k_spread<4, float>, nb, kIbmThreads, 0, s, a);
+    launch_chained(k_spread<2, float>, nb, kIbmThreads, 0, s, a);
+  }
+  LBM_LAUNCH_CHECK("ibm_spread_claimed");
+  return LBM_OK;
 }
 
 int rigid_step(const lbm_particles *pt, float dt, float gl, float rouf, void *stream) {
@@ -1138,9 +1280,9 @@ int rigid_step(const lbm_particles *pt, float dt, float gl, float rouf, void *st
   a.gl = gl;
   a.rouf = rouf;
   if (pt->fp64)
-    k_rigid_step<double><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
+    launch_chained(k_rigid_step<double>, pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream, a);
   else
-    k_rigid_step<float><<<pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream>>>(a);
+    launch_chained(k_rigid_step<float>, pt->n_particles, kRigidThreads, 0, (cudaStream_t)stream, a);
   LBM_LAUNCH_CHECK("rigid_step");
   return LBM_OK;
 }
@@ -1207,9 +1349,9 @@ int ibm_spread_tiled(const lbm_lattice *lat, const lbm_particles *pt, int32_t mo
   const bool fp64 = lat->storage == LBM_STORAGE_FP64;
   const long long nchunks = (a.g.n + 31) >> 5;
   if (fp64)
-    k_spread_clear<double><<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, (double *)field, chunks);
+    launch_chained(k_spread_clear<double>, blocks_for(nchunks, 256), 256, 0, s, a.g.n, (double *)field, chunks);
   else
-    k_spread_clear<float><<<blocks_for(nchunks, 256), 256, 0, s>>>(a.g.n, field, chunks);
+    launch_chained(k_spread_clear<float>, blocks_for(nchunks, 256), 256, 0, s, a.g.n, field, chunks);
   LBM_LAUNCH_CHECK("ibm_spread_tiled");
   if (pt->n_markers == 0) return LBM_OK;
   const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);

@@ -31,6 +31,27 @@ __device__ __forceinline__ bool lbm_in(bool ok) {
 __device__ __forceinline__ constexpr bool lbm_in(bool) { return true; }
 #endif
 
+// Chained launches (programmatic dependent launch).  The kernels of one
+// lattice step -- interpolation, spreading, the rigid update and the fused
+// step -- are launched with programmatic stream serialization
+// (launch_chained): the GPU may schedule such a kernel while the kernel
+// before it in the stream is still running.  chain_wait() is therefore the
+// first statement of each of them, executed by every thread before any
+// memory access: it returns once the previous kernel has completed and its
+// writes are visible, so every access happens in plain stream order.
+// chain_release() right after it lets the next kernel be scheduled while
+// this one runs (a kernel is only scheduled once every block of the one
+// before it has started, so a waiting kernel never holds resources the
+// running one still needs).  Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void chain_release() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void chain_enter() {
+  chain_wait();
+  chain_release();
+}
+
 // Compile-time loop: calls fn(std::integral_constant<int, I>) for I < N, so
 // every population index is a constant and f[Q] stays in registers.
 template <typename F, int... I>

@@ -250,6 +250,7 @@ constexpr int scalar_min_blocks() {
 
 template <int Q, int S, bool FORCE>
 __global__ void __launch_bounds__(kThreads, (scalar_min_blocks<Q, S>())) k_step(const __grid_constant__ StepArgs a) {
+  chain_enter();
   step_scalar_body<Q, S, FORCE>(a, blockIdx.x * kThreads + threadIdx.x);
 }
 
@@ -735,6 +736,7 @@ constexpr int vec_min_blocks() {
 template <int Q, int S, bool FORCE, int NZ, int TB, bool PITCH>
 __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>()))
     k_step_vec(const __grid_constant__ StepArgs a) {
+  chain_enter();
   step_vec_body<Q, S, FORCE, NZ, PITCH>(a, blockIdx.x * TB + threadIdx.x);
 }
 
@@ -747,6 +749,7 @@ __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, NZ, TB, FORCE>()))
 template <int Q, int S, bool FORCE, int TB>
 __global__ void __launch_bounds__(TB, (vec_min_blocks<Q, S, 2, TB, FORCE>()))
     k_step_odd(const __grid_constant__ StepArgs a, const FastDiv per_row, unsigned rows) {
+  chain_enter();
   const unsigned t = blockIdx.x * TB + threadIdx.x;
   const unsigned row = fdiv(t, per_row);
   if (row >= rows) return;
@@ -1101,14 +1104,14 @@ struct StepLauncher {
     const unsigned nb = blocks_for(a.g.np / NZ, TB);
     if (a.g.pz != a.g.nz) {
       if (force)
-        k_step_vec<Q, S, true, NZ, TB, true><<<nb, TB, 0, s>>>(a);
+        launch_chained(k_step_vec<Q, S, true, NZ, TB, true>, nb, TB, 0, s, a);
       else
-        k_step_vec<Q, S, false, NZ, TB, true><<<nb, TB, 0, s>>>(a);
+        launch_chained(k_step_vec<Q, S, false, NZ, TB, true>, nb, TB, 0, s, a);
     } else {
       if (force)
-        k_step_vec<Q, S, true, NZ, TB, false><<<nb, TB, 0, s>>>(a);
+        launch_chained(k_step_vec<Q, S, true, NZ, TB, false>, nb, TB, 0, s, a);
       else
-        k_step_vec<Q, S, false, NZ, TB, false><<<nb, TB, 0, s>>>(a);
+        launch_chained(k_step_vec<Q, S, false, NZ, TB, false>, nb, TB, 0, s, a);
     }
   }
   template <int NZ>
@@ -1124,7 +1127,7 @@ struct StepLauncher {
       const unsigned per_row = (unsigned)(a.g.nz + 1) / 2;
       const unsigned rows = (unsigned)(a.g.nx * a.g.ny);
       const unsigned nb = blocks_for((long long)rows * per_row, TB);
-      k_step_odd<Q, S, FORCE, TB><<<nb, TB, 0, s>>>(a, make_fastdiv(per_row), rows);
+      launch_chained(k_step_odd<Q, S, FORCE, TB>, nb, TB, 0, s, a, make_fastdiv(per_row), rows);
     }
   }
   static void go_odd(const StepArgs &a, bool force, int threads, cudaStream_t s) {
@@ -1174,9 +1177,9 @@ struct StepLauncher {
     }
     const unsigned nb = blocks_for(a.g.n, kThreads);
     if (force)
-      k_step<Q, S, true><<<nb, kThreads, 0, s>>>(a);
+      launch_chained(k_step<Q, S, true>, nb, kThreads, 0, s, a);
     else
-      k_step<Q, S, false><<<nb, kThreads, 0, s>>>(a);
+      launch_chained(k_step<Q, S, false>, nb, kThreads, 0, s, a);
     return LBM_OK;
   }
 };

@@ -474,18 +474,29 @@ class LBMD3(LBMBase):
         if not launch:
             return plan
         dt = float(self.config.dt)
+        mode = 0 if self.config.ibm_mode == "reference" else 1
+        # reference-mode spreading with global claims: the claims and the
+        # clearing of the buffer ride in the interpolation's launch
+        claimed = bool(parts) and mode == 0 and self.config.ibm_spread != "tiles"
         if parts:
             sw = self.particle_swarm
             sw.ensure_extremes()
             st = ctypes.byref(sw.struct())
             f_int = make_force(old_uniform=g_old, old_field=F_old)
             # flow_to_lagrange and particle_to_wall in one launch
-            call("ibm_interpolate_wall", ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]),
-                 ctypes_ref(f_int), ptr(lat.face_rho[lat.cur]), st, dt, float(self.config.dx),
-                 int(self.step), ptr(self._status_ibm), s)
-        mode = 0 if self.config.ibm_mode == "reference" else 1
+            args = (ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]), ctypes_ref(f_int),
+                    ptr(lat.face_rho[lat.cur]), st, dt, float(self.config.dx), int(self.step),
+                    ptr(self._status_ibm))
+            if claimed:
+                call("ibm_interpolate_wall_claim", *args, ptr(F_new), ptr(C_new),
+                     ptr(self._owner), s)
+            else:
+                call("ibm_interpolate_wall", *args, s)
         sw_struct = self.particle_swarm.struct() if parts else _empty_particles()
-        if self.config.ibm_spread == "tiles":
+        if claimed:
+            call("ibm_spread_claimed", ctypes_ref(lat.desc), ctypes.byref(sw_struct), ptr(F_new),
+                 ptr(C_new), ptr(self._owner), s)
+        elif self.config.ibm_spread == "tiles":
             call("ibm_spread_tiled", ctypes_ref(lat.desc), ctypes.byref(sw_struct), mode,
                  ptr(F_new), ptr(C_new), ptr(self._spread_scratch), self._spread_scratch.numel(),
                  s)

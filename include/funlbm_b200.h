@@ -318,6 +318,27 @@ int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force
                          const float *face_rho_in, const lbm_particles *pt, float dt, float dx,
                          int32_t step, uint32_t *status, void *stream);
 
+/* LBMD3.flow_to_lagrange + particle_to_wall + the first half of
+ * lagrange_to_flow in reference mode (lbm/lbm3d.py:66-119): ibm_interpolate_wall,
+ * and in the same launch the claims of ibm_spread's reference mode (every
+ * in-box stencil node of every marker gets the largest marker index in
+ * `owner`, which must hold -1 there) and the clearing of the chunks of `field`
+ * flagged in `chunks` (those written the last time this buffer was used).
+ * ibm_spread_claimed finishes the spreading; the pair gives the results of
+ * ibm_interpolate_wall followed by ibm_spread(mode 0) in two launches fewer.
+ * With no markers only the clearing runs. */
+int ibm_interpolate_wall_claim(const lbm_lattice *lat, const void *fa, const lbm_force *force,
+                               const float *face_rho_in, const lbm_particles *pt, float dt,
+                               float dx, int32_t step, uint32_t *status, float *field,
+                               uint8_t *chunks, int32_t *owner, void *stream);
+
+/* The second half of reference-mode LBMD3.lagrange_to_flow
+ * (lbm/lbm3d.py:102-119) after ibm_interpolate_wall_claim: the owner of each
+ * claimed node writes w lF lm there and flags its chunk, then the claims are
+ * released (`owner` holds -1 again). */
+int ibm_spread_claimed(const lbm_lattice *lat, const lbm_particles *pt, float *field,
+                       uint8_t *chunks, int32_t *owner, void *stream);
+
 /* Particle.update_from_lar then Particle.update (particle/base/base.py:120-156,
  * particle/coord.py:87-108) for all particles in one launch -- the rigid
  * update of rigid_wall_and_update(RIGID_UPDATE) followed by the marker

@@ -266,6 +266,64 @@ def test_fused_particle_calls_match_separate_calls(storage):
         assert np.array_equal(a, b), (k, np.abs(a - b).max(), spring)
 
 
+@pytest.mark.parametrize("storage", ["fp32", "fp64"])
+def test_claiming_interpolation_matches_interpolation_and_spread(storage):
+    """ibm_interpolate_wall_claim + ibm_spread_claimed (the driver's calls in
+    reference mode) against ibm_interpolate_wall + ibm_spread(mode 0): the
+    same marker forces and velocities, field and chunk flags bit for bit, and
+    the claim array back at -1, on two calls in a row (the second clears what
+    the first wrote, after the particles have moved).  Particles touch the
+    walls, so the spring and stencils cut by the lattice's faces take part."""
+    import ctypes
+
+    from funlbm_b200._lib import call, ptr
+    from funlbm_b200.lattice import ctypes_ref, make_force
+
+    dt = torch.float64 if storage == "fp64" else torch.float32
+    parts = [{"type": "sphere", "r": 3, "rou": 1.4, "coord": {"center": [2.2, 8.0, 9.1]}},
+             {"type": "ellipsoid", "a": 3, "b": 2, "c": 2.5, "rou": 0.7,
+              "coord": {"center": [14.5, 13.3, 1.6], "alpha": 0.3, "beta": -0.5, "gamma": 0.2}},
+             {"type": "sphere", "r": 2, "rou": 1.1, "coord": {"center": [9.0, 6.0, 9.0]}}]
+    lbm = LBMD3_with(parts, storage)
+    lat = lbm.flow.lattice
+    sw = lbm.particle_swarm
+    sw.update()
+    n = lat.n
+    nch = (n + 31) // 32
+    bufs = {v: (torch.zeros(3 * n, device="cuda", dtype=dt),
+                torch.zeros(nch, dtype=torch.uint8, device="cuda"),
+                torch.full((n,), -1, dtype=torch.int32, device="cuda"))
+            for v in ("plain", "claimed")}
+    force = make_force()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = lat.stream()
+    for rep in range(2):
+        if rep:
+            sw.cx.add_(torch.tensor([0.37, -0.21, 0.44], device="cuda", dtype=dt))
+            sw.update()
+        out = {}
+        for v in ("plain", "claimed"):
+            field, chunks, owner = bufs[v]
+            st = ctypes.byref(sw.struct())
+            call("rigid_extremes", st, s)
+            args = (ctypes_ref(lat.desc), ptr(lat.buf[lat.cur]), ctypes_ref(force),
+                    ptr(lat.face_rho[lat.cur]), st, 1.0, 1.0, 5, ptr(status))
+            if v == "plain":
+                call("ibm_interpolate_wall", *args, s)
+                call("ibm_spread", ctypes_ref(lat.desc), st, 0, ptr(field), ptr(chunks),
+                     ptr(owner), s)
+            else:
+                call("ibm_interpolate_wall_claim", *args, ptr(field), ptr(chunks), ptr(owner), s)
+                call("ibm_spread_claimed", ctypes_ref(lat.desc), st, ptr(field), ptr(chunks),
+                     ptr(owner), s)
+            torch.cuda.synchronize()
+            out[v] = [t.cpu().numpy().copy() for t in (sw.lF, sw.lu, field, chunks, owner)]
+        assert np.abs(out["plain"][2]).max() > 0
+        for k, (a, b) in enumerate(zip(out["plain"], out["claimed"])):
+            assert np.array_equal(a, b), (rep, k)
+        assert (out["claimed"][4] == -1).all()
+
+
 def LBMD3_with(parts, storage):
     from funlbm_b200.lbm import LBMD3
 
