@@ -321,6 +321,23 @@ __device__ __forceinline__ void rigid_update_block(const RigidArgs &a, const PVi
                                                    double (*s_sum)[kRigidThreads / 32], R *s_cx,
                                                    R *s_ang) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // Thread 0's particle state, loaded before the marker sums: the update
+  // below interleaves its stores with these reads, which would otherwise
+  // each wait out a memory round trip after the barrier.  Nothing in this
+  // block writes them before the update.
+  R p_mass = R(0), p_rou = R(0), p_cu[3] = {}, p_cx[3] = {}, p_cw[3] = {}, p_in[3] = {},
+    p_ang[3] = {};
+  if (threadIdx.x == 0) {
+    p_mass = P.mass[pi];
+    p_rou = P.rou[pi];
+    for (int k = 0; k < 3; ++k) {
+      p_cu[k] = P.cu[3 * pi + k];
+      p_cx[k] = P.cx[3 * pi + k];
+      p_cw[k] = P.cw[3 * pi + k];
+      p_in[k] = P.inertia[3 * pi + k];
+      if (s_ang != nullptr) p_ang[k] = P.angle[3 * pi + k];
+    }
+  }
   double sm[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   // (unrolled so that the loads of several markers are in flight together;
   // the sums keep their marker order)
@@ -352,15 +369,15 @@ __device__ __forceinline__ void rigid_update_block(const RigidArgs &a, const PVi
         B[k] += s_sum[k + 3][w];
       }
     }
-    const R mass = P.mass[pi];
-    const R buoy = (R)(1.0 - (double)P.rou[pi] / (double)a.rouf) * mass;
+    const R mass = p_mass;
+    const R buoy = (R)(1.0 - (double)p_rou / (double)a.rouf) * mass;
     double c[3];
     for (int k = 0; k < 3; ++k) {
       const R cf = (R)(-A[k]) + (k == 0 ? buoy * (R)a.gl : R(0));
       P.cF[3 * pi + k] = cf;
-      const R cu = P.cu[3 * pi + k] + cf / mass * (R)a.dt;
+      const R cu = p_cu[k] + cf / mass * (R)a.dt;
       P.cu[3 * pi + k] = cu;
-      const R cx = P.cx[3 * pi + k] + cu * (R)a.dt;
+      const R cx = p_cx[k] + cu * (R)a.dt;
       P.cx[3 * pi + k] = cx;
       s_cx[k] = cx;
       c[k] = (double)cx;
@@ -370,12 +387,12 @@ __device__ __forceinline__ void rigid_update_block(const RigidArgs &a, const PVi
     for (int k = 0; k < 3; ++k) {
       const R ct = -(R)T[k];
       P.cT[3 * pi + k] = ct;
-      const R cw = P.cw[3 * pi + k] + R(0.1) * ct * (R)a.dt / P.inertia[3 * pi + k];
+      const R cw = p_cw[k] + R(0.1) * ct * (R)a.dt / p_in[k];
       P.cw[3 * pi + k] = cw;
       if (s_ang != nullptr) {
         // shared, so that no thread reads the rotation vector after it is
         // overwritten
-        const R ang = P.angle[3 * pi + k] + cw;
+        const R ang = p_ang[k] + cw;
         s_ang[k] = ang;
         P.angle[3 * pi + k] = ang;
       }
