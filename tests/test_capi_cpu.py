@@ -138,3 +138,23 @@ def test_normal_build_has_no_bounds_counters(lib):
     """Only the bounds-checked build (FUNLBM_B200_CHECKED=1) counts index
     violations; the normal library says so with -1."""
     assert lib.lbm_debug_bounds_faults(0) == -1
+
+
+def test_claiming_spread_pair_rejects_missing_buffers(lib):
+    """ibm_interpolate_wall_claim / ibm_spread_claimed validate their
+    arguments before touching the device: without the field, chunk flags or
+    claim array they return LBM_ERR_INVALID with a message naming the call."""
+    lat = _desc()
+    pt = _lib.LbmParticles()
+    dummy = ctypes.c_void_p(16)      # never dereferenced: validation fails first
+    rc = lib.ibm_interpolate_wall_claim(ctypes.byref(lat), dummy, None, None, ctypes.byref(pt),
+                                        1.0, 1.0, 0, None, dummy, None, dummy, None)
+    assert rc == _lib.LBM_ERR_INVALID
+    assert b"ibm_interpolate_wall_claim" in lib.lbm_last_error()
+    rc = lib.ibm_spread_claimed(ctypes.byref(lat), ctypes.byref(pt), dummy, dummy, None, None)
+    assert rc == _lib.LBM_ERR_INVALID
+    assert b"ibm_spread_claimed" in lib.lbm_last_error()
+    rc = lib.ibm_interpolate_wall_claim(ctypes.byref(lat), dummy, None, None, ctypes.byref(pt),
+                                        0.0, 1.0, 0, None, dummy, dummy, dummy, None)
+    assert rc == _lib.LBM_ERR_INVALID
+    assert b"dt must be positive" in lib.lbm_last_error()
