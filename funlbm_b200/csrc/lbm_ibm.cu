@@ -504,7 +504,10 @@ struct SpreadArgs {
 // pass 3: accumulate w lF lm (accumulate mode; flags set as in pass 0)
 // pass 4: pass 1 after claims made by ibm_interpolate_wall_claim -- the owner
 //         also flags the chunk (every claimed node has exactly one owner, so
-//         the flagged chunks are pass 0's)
+//         the flagged chunks are pass 0's) and releases its claim (pass 2's
+//         work: a thread of another marker that reads the node's claim after
+//         the release sees -1, which is not its index either, so it still
+//         leaves the node to the owner)
 template <int PASS, typename R>
 __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
   chain_enter();
@@ -544,7 +547,10 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
   const R lm = P.lm[m];
   if (PASS == 1 || PASS == 4) {
     if (a.owner[idx] != m) return;
-    if (PASS == 4) a.chunks[idx >> 5] = 1;
+    if (PASS == 4) {
+      a.owner[idx] = -1;
+      a.chunks[idx >> 5] = 1;
+    }
     for (int k = 0; k < 3; ++k) field[3 * idx + k] = (wn * P.lF[3 * m + k]) * lm;
   } else {
     a.chunks[idx >> 5] = 1;
@@ -1265,13 +1271,10 @@ int ibm_spread_claimed(const lbm_lattice *lat, const lbm_particles *pt, float *f
   a.chunks = chunks;
   a.owner = owner;
   const unsigned nb = (unsigned)((pt->n_markers + kMarkersPerBlock - 1) / kMarkersPerBlock);
-  if (lat->storage == LBM_STORAGE_FP64) {
+  if (lat->storage == LBM_STORAGE_FP64)
     launch_chained(k_spread<4, double>, nb, kIbmThreads, 0, s, a);
-    launch_chained(k_spread<2, double>, nb, kIbmThreads, 0, s, a);
-  } else {
+  else
     launch_chained(k_spread<4, float>, nb, kIbmThreads, 0, s, a);
-    launch_chained(k_spread<2, float>, nb, kIbmThreads, 0, s, a);
-  }
   LBM_LAUNCH_CHECK("ibm_spread_claimed");
   return LBM_OK;
 }

@@ -325,7 +325,7 @@ int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force
  * `owner`, which must hold -1 there) and the clearing of the chunks of `field`
  * flagged in `chunks` (those written the last time this buffer was used).
  * ibm_spread_claimed finishes the spreading; the pair gives the results of
- * ibm_interpolate_wall followed by ibm_spread(mode 0) in two launches fewer.
+ * ibm_interpolate_wall followed by ibm_spread(mode 0) in three launches fewer.
  * With no markers only the clearing runs. */
 int ibm_interpolate_wall_claim(const lbm_lattice *lat, const void *fa, const lbm_force *force,
                                const float *face_rho_in, const lbm_particles *pt, float dt,
@@ -333,9 +333,9 @@ int ibm_interpolate_wall_claim(const lbm_lattice *lat, const void *fa, const lbm
                                uint8_t *chunks, int32_t *owner, void *stream);
 
 /* The second half of reference-mode LBMD3.lagrange_to_flow
- * (lbm/lbm3d.py:102-119) after ibm_interpolate_wall_claim: the owner of each
- * claimed node writes w lF lm there and flags its chunk, then the claims are
- * released (`owner` holds -1 again). */
+ * (lbm/lbm3d.py:102-119) after ibm_interpolate_wall_claim, in one launch: the
+ * owner of each claimed node writes w lF lm there, flags its chunk and
+ * releases the claim (`owner` holds -1 again afterwards). */
 int ibm_spread_claimed(const lbm_lattice *lat, const lbm_particles *pt, float *field,
                        uint8_t *chunks, int32_t *owner, void *stream);
 
