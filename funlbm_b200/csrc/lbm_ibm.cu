@@ -499,15 +499,15 @@ struct SpreadArgs {
 };
 
 // pass 0: flag chunks and claim nodes (max marker index = last in loop order)
-// pass 1: the owning marker writes w lF lm (reference mode)
-// pass 2: release the claims
+// pass 1: the owning marker writes w lF lm (reference mode) and releases its
+//         claim: a thread of another marker that reads the node's claim after
+//         the release sees -1, which is not its index either, so it still
+//         leaves the node to the owner, and the claim array holds -1 again
+//         when the pass ends
 // pass 3: accumulate w lF lm (accumulate mode; flags set as in pass 0)
 // pass 4: pass 1 after claims made by ibm_interpolate_wall_claim -- the owner
 //         also flags the chunk (every claimed node has exactly one owner, so
-//         the flagged chunks are pass 0's) and releases its claim (pass 2's
-//         work: a thread of another marker that reads the node's claim after
-//         the release sees -1, which is not its index either, so it still
-//         leaves the node to the owner)
+//         the flagged chunks are pass 0's)
 template <int PASS, typename R>
 __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
   chain_enter();
@@ -529,14 +529,10 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
   }
   const long long idx = ((long long)x * a.g.ny + y) * a.g.nz + z;
   if (in_box && !lbm_in(idx >= 0 && idx < a.g.n)) in_box = false;
-  if (PASS == 0 || PASS == 2) {
+  if (PASS == 0) {
     if (!in_box) return;
-    if (PASS == 0) {
-      a.chunks[idx >> 5] = 1;
-      atomicMax(a.owner + idx, m);
-    } else {
-      a.owner[idx] = -1;
-    }
+    a.chunks[idx >> 5] = 1;
+    atomicMax(a.owner + idx, m);
     return;
   }
   // passes 1 and 3 need the normalised weight: sum over the marker's stencil
@@ -547,10 +543,8 @@ __global__ void __launch_bounds__(kIbmThreads) k_spread(const SpreadArgs a) {
   const R lm = P.lm[m];
   if (PASS == 1 || PASS == 4) {
     if (a.owner[idx] != m) return;
-    if (PASS == 4) {
-      a.owner[idx] = -1;
-      a.chunks[idx >> 5] = 1;
-    }
+    a.owner[idx] = -1;
+    if (PASS == 4) a.chunks[idx >> 5] = 1;
     for (int k = 0; k < 3; ++k) field[3 * idx + k] = (wn * P.lF[3 * m + k]) * lm;
   } else {
     a.chunks[idx >> 5] = 1;
@@ -950,8 +944,8 @@ static int check_precision(const lbm_lattice *lat, const lbm_particles *pt, cons
   return LBM_OK;
 }
 
-// spreading launches (clear, then the claim / write / release passes or the
-// accumulation) in the particles' arithmetic type
+// spreading launches (clear, then the claim pass and the write pass that
+// releases the claims, or the accumulation) in the particles' arithmetic type
 template <typename R>
 static int spread_launch(const SpreadArgs &a, int mode, long long n_markers, cudaStream_t s,
                          const char *who) {
@@ -964,7 +958,6 @@ static int spread_launch(const SpreadArgs &a, int mode, long long n_markers, cud
   if (mode == 0) {
     launch_chained(k_spread<0, R>, nb, kIbmThreads, 0, s, a);
     launch_chained(k_spread<1, R>, nb, kIbmThreads, 0, s, a);
-    launch_chained(k_spread<2, R>, nb, kIbmThreads, 0, s, a);
   } else {
     launch_chained(k_spread<3, R>, nb, kIbmThreads, 0, s, a);
   }
@@ -1440,7 +1433,7 @@ int ibm_spread_noalloc(const lbm_lattice *lat, const lbm_particles *pt, int32_t 
   a.owner = owner;
   const bool claims = mode == 0 && pt->n_markers > 0;
   if (claims) {
-    // the claim passes need -1 in every slot they touch; the release pass
+    // the claim pass needs -1 in every slot it touches; the write pass
     // restores it, so only the first reference-mode call on a device (or
     // one after a failed call) resets the whole array
     owner_mark(dev, false);

@@ -325,7 +325,7 @@ int ibm_interpolate_wall(const lbm_lattice *lat, const void *fa, const lbm_force
  * `owner`, which must hold -1 there) and the clearing of the chunks of `field`
  * flagged in `chunks` (those written the last time this buffer was used).
  * ibm_spread_claimed finishes the spreading; the pair gives the results of
- * ibm_interpolate_wall followed by ibm_spread(mode 0) in three launches fewer.
+ * ibm_interpolate_wall followed by ibm_spread(mode 0) in two launches fewer.
  * With no markers only the clearing runs. */
 int ibm_interpolate_wall_claim(const lbm_lattice *lat, const void *fa, const lbm_force *force,
                                const float *face_rho_in, const lbm_particles *pt, float dt,
